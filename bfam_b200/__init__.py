@@ -1,0 +1,430 @@
+"""bfam_b200: B200 device layer for bfam's DG elastic right-hand side and LSRK
+step, with a host front end that produces bfam's volume/glue data model.
+
+Python here is a thin mirror over the C-ABI in ``include/bfam_gpu.h`` and
+``include/bfam_b200_host.h`` (ctypes, no torch).  The compute path is the
+CUDA library ``libbfam_b200.so``; if it is missing, importing this module
+raises -- there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libbfam_b200.so"
+
+FIELDS_2D = ("vx", "vy", "sxx", "syy", "sxy")
+FIELDS_3D = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
+
+FLUX_UPWIND, FLUX_CENTRAL = 0, 1
+PRECISION_FP64, PRECISION_FP32 = 0, 1
+LSRK_KC54, LSRK_FE, LSRK_HEUN, LSRK_W33 = 0, 1, 2, 3
+
+
+class BfamGpuError(RuntimeError):
+    """Raised when a bfam_gpu_* call returns a nonzero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bfam_gpu error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m bfam_b200.build` "
+                "(the CUDA library is required; there is no CPU fallback)")
+        _lib = C.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+P = C.POINTER
+i8p, i32p, dp = P(C.c_int8), P(C.c_int32), P(C.c_double)
+
+
+class BrickSpec(C.Structure):
+    _fields_ = [("dim", C.c_int), ("N", C.c_int), ("n", C.c_int * 3),
+                ("L", C.c_double * 3), ("periodic", C.c_int * 3),
+                ("refine_prob", C.c_double), ("seed", C.c_uint64),
+                ("refine_flags", P(C.c_uint8))]
+
+
+class MeshStruct(C.Structure):
+    _fields_ = [("dim", C.c_int), ("N", C.c_int), ("Nq", C.c_int), ("Np", C.c_int),
+                ("Nfp", C.c_int), ("Nfaces", C.c_int), ("K", C.c_int32),
+                ("ecoord", i32p), ("x0", dp), ("h", dp),
+                ("EToE", i32p), ("EToF", i8p), ("vmapM", i32p), ("vmapP", i32p),
+                ("Kg", C.c_int32), ("EToEm", i32p), ("EToFm", i8p), ("EToHm", i8p),
+                ("EToEp", i32p), ("EToHp", i8p), ("EToOp", i8p),
+                ("num_refined", C.c_int32)]
+
+
+class VolumeDesc(C.Structure):
+    _fields_ = [("dim", C.c_int), ("N", C.c_int), ("K", C.c_int32),
+                ("r", dp), ("w", dp), ("Dr", dp), ("vmapM", i32p), ("vmapP", i32p),
+                ("x0", dp), ("h", dp), ("rho", dp), ("lambda_", dp), ("mu", dp)]
+
+
+class GlueDesc(C.Structure):
+    _fields_ = [("K", C.c_int32), ("EToEp", i32p), ("EToHp", i8p), ("EToOp", i8p),
+                ("EToEm", i32p), ("EToFm", i8p), ("EToHm", i8p),
+                ("interpolation", dp * 3), ("projection", dp * 3)]
+
+
+class Options(C.Structure):
+    _fields_ = [("flux", C.c_int), ("precision", C.c_int),
+                ("mem_budget_bytes", C.c_size_t), ("device", C.c_int)]
+
+
+def _declare(L: C.CDLL) -> None:
+    vp = C.c_void_p
+    sig = {
+        "bfam_b200_brick_mesh_new": (C.c_int, [P(BrickSpec), P(P(MeshStruct))]),
+        "bfam_b200_brick_mesh_free": (None, [P(MeshStruct)]),
+        "bfam_b200_lgl_operators": (C.c_int, [C.c_int, dp, dp, dp, dp]),
+        "bfam_b200_mortar_operators": (C.c_int, [C.c_int, C.c_int, dp]),
+        "bfam_b200_lsrk_coefficients": (C.c_int, [C.c_int, dp, dp, dp]),
+        "bfam_b200_material_random": (None, [C.c_int32, C.c_uint64, C.c_double, C.c_double,
+                                              C.c_double, C.c_double, C.c_double,
+                                              C.c_double, dp, dp, dp]),
+        "bfam_b200_node_coordinates": (None, [P(MeshStruct), dp, dp, dp, dp]),
+        "bfam_b200_init_plane_wave": (None, [P(MeshStruct), dp, dp, C.c_double, C.c_double,
+                                              C.c_double, C.c_double, C.c_double, P(dp)]),
+        "bfam_b200_init_gaussian_pulse": (None, [P(MeshStruct), dp, dp, C.c_double, P(dp)]),
+        "bfam_b200_pcg32_seed": (None, [vp, C.c_uint64, C.c_uint64]),
+        "bfam_b200_pcg32_next": (C.c_uint32, [vp]),
+        "bfam_b200_pcg32_bounded": (C.c_uint32, [vp, C.c_uint32]),
+        "bfam_b200_pcg32_uniform": (C.c_double, [vp]),
+        "bfam_gpu_domain_create": (C.c_int, [P(VolumeDesc), P(GlueDesc), P(Options), P(vp)]),
+        "bfam_gpu_domain_free": (C.c_int, [vp]),
+        "bfam_gpu_domain_num_fields": (C.c_int, [vp]),
+        "bfam_gpu_domain_field_length": (C.c_size_t, [vp]),
+        "bfam_gpu_domain_device_bytes": (C.c_size_t, [vp]),
+        "bfam_gpu_domain_set_fields": (C.c_int, [vp, P(dp)]),
+        "bfam_gpu_domain_get_fields": (C.c_int, [vp, P(dp)]),
+        "bfam_gpu_domain_rhs": (C.c_int, [vp, P(dp)]),
+        "bfam_gpu_domain_energy": (C.c_int, [vp, dp]),
+        "bfam_gpu_domain_field_device_ptr": (vp, [vp, C.c_int]),
+        "bfam_gpu_domain_set_stream": (C.c_int, [vp, vp]),
+        "bfam_gpu_domain_sync": (C.c_int, [vp]),
+        "bfam_ts_lsrk_init": (C.c_int, [P(vp), vp, C.c_int, C.c_double]),
+        "bfam_ts_lsrk_step": (C.c_int, [vp, C.c_double, C.c_int, C.c_int]),
+        "bfam_ts_lsrk_time": (C.c_int, [vp, dp]),
+        "bfam_ts_lsrk_free": (C.c_int, [vp]),
+        "bfam_gpu_launch_count": (C.c_uint64, []),
+        "bfam_gpu_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().bfam_gpu_last_error(buf, 1024)
+    return buf.value.decode()
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise BfamGpuError(rc, last_error())
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(dp)
+
+
+def _ptrs(arrs) -> C.Array:
+    return (dp * len(arrs))(*[_dp(a) for a in arrs])
+
+
+def launch_count() -> int:
+    return int(lib().bfam_gpu_launch_count())
+
+
+# ----------------------------------------------------------------- operators
+
+def lgl_operators(N: int):
+    """r, w, wi, Dr (column-major flat) for order N."""
+    n = N + 1
+    r, w, wi, D = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(n * n)
+    if lib().bfam_b200_lgl_operators(N, _dp(r), _dp(w), _dp(wi), _dp(D)):
+        raise ValueError(f"bad order {N}")
+    return r, w, wi, D
+
+
+def mortar_operators(N_src: int, N_dst: int) -> np.ndarray:
+    """(5, (N_dst+1)*(N_src+1)) column-major: same, cfb, cft, r2b, r2t."""
+    n = (N_src + 1) * (N_dst + 1)
+    out = np.zeros(5 * n)
+    if lib().bfam_b200_mortar_operators(N_src, N_dst, _dp(out)):
+        raise ValueError("bad orders")
+    return out.reshape(5, n)
+
+
+def lsrk_coefficients(method: int = LSRK_KC54):
+    A, B, Cc = np.zeros(6), np.zeros(6), np.zeros(7)
+    ns = lib().bfam_b200_lsrk_coefficients(method, _dp(A), _dp(B), _dp(Cc))
+    if ns < 0:
+        raise ValueError(f"unknown LSRK method {method}")
+    return A[:ns].copy(), B[:ns].copy(), Cc[:ns + 1].copy()
+
+
+class PCG32:
+    """The PCG32 stream used for every seeded draw."""
+
+    def __init__(self, seed: int, seq: int):
+        self._st = (C.c_uint64 * 2)()
+        lib().bfam_b200_pcg32_seed(C.cast(self._st, C.c_void_p), seed, seq)
+
+    def next(self) -> int:
+        return int(lib().bfam_b200_pcg32_next(C.cast(self._st, C.c_void_p)))
+
+    def bounded(self, bound: int) -> int:
+        return int(lib().bfam_b200_pcg32_bounded(C.cast(self._st, C.c_void_p), bound))
+
+    def uniform(self) -> float:
+        return float(lib().bfam_b200_pcg32_uniform(C.cast(self._st, C.c_void_p)))
+
+
+# ---------------------------------------------------------------------- mesh
+
+class Mesh:
+    """Brick mesh in bfam's data model (see bfam_b200_brick_mesh_new)."""
+
+    def __init__(self, dim: int, N: int, n, L=(1.0, 1.0, 1.0), refine_prob: float = 0.0,
+                 seed: int = 0, refine_flags=None):
+        spec = BrickSpec()
+        spec.dim, spec.N = dim, N
+        nn = list(n) + [1] * (3 - len(n))
+        LL = list(L) + [1.0] * (3 - len(L))
+        for a in range(3):
+            spec.n[a] = int(nn[a])
+            spec.L[a] = float(LL[a])
+            spec.periodic[a] = 1
+        spec.refine_prob = float(refine_prob)
+        spec.seed = int(seed)
+        self._flags = None
+        if refine_flags is not None:
+            self._flags = np.ascontiguousarray(refine_flags, dtype=np.uint8)
+            spec.refine_flags = self._flags.ctypes.data_as(P(C.c_uint8))
+        ptr = P(MeshStruct)()
+        rc = lib().bfam_b200_brick_mesh_new(C.byref(spec), C.byref(ptr))
+        if rc:
+            raise ValueError(f"bfam_b200_brick_mesh_new failed ({rc})")
+        self._ptr = ptr
+        m = ptr.contents
+        self.dim, self.N, self.Nq, self.Np = m.dim, m.N, m.Nq, m.Np
+        self.Nfp, self.Nfaces, self.K, self.Kg = m.Nfp, m.Nfaces, m.K, m.Kg
+        self.nbase = tuple(nn[:3])
+        self.L = tuple(LL[:3])
+        self.num_refined = m.num_refined
+        K, NF, Nfp, Kg = self.K, self.Nfaces, self.Nfp, self.Kg
+
+        def arr(p, n, dt):
+            return np.ctypeslib.as_array(p, shape=(n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+
+        self.ecoord = arr(m.ecoord, 4 * K, np.int32).reshape(K, 4)
+        self.x0 = arr(m.x0, 3 * K, np.float64).reshape(K, 3)
+        self.h = arr(m.h, 3 * K, np.float64).reshape(K, 3)
+        self.EToE = arr(m.EToE, NF * K, np.int32).reshape(K, NF)
+        self.EToF = arr(m.EToF, NF * K, np.int8).reshape(K, NF)
+        self.vmapM = arr(m.vmapM, K * NF * Nfp, np.int32)
+        self.vmapP = arr(m.vmapP, K * NF * Nfp, np.int32)
+        self.EToEm = arr(m.EToEm, Kg, np.int32)
+        self.EToFm = arr(m.EToFm, Kg, np.int8)
+        self.EToHm = arr(m.EToHm, Kg, np.int8)
+        self.EToEp = arr(m.EToEp, Kg, np.int32)
+        self.EToHp = arr(m.EToHp, Kg, np.int8)
+        self.EToOp = arr(m.EToOp, Kg, np.int8)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_ptr", None):
+                lib().bfam_b200_brick_mesh_free(self._ptr)
+                self._ptr = None
+        except Exception:
+            pass
+
+    @property
+    def nfields(self) -> int:
+        return 9 if self.dim == 3 else 5
+
+    @property
+    def ndof(self) -> int:
+        return self.K * self.Np * self.nfields
+
+    def node_coordinates(self, r):
+        n = self.K * self.Np
+        x, y, z = np.zeros(n), np.zeros(n), np.zeros(n)
+        lib().bfam_b200_node_coordinates(self._ptr, _dp(np.ascontiguousarray(r)),
+                                         _dp(x), _dp(y), _dp(z))
+        return x, y, z
+
+    def empty_fields(self) -> np.ndarray:
+        return np.zeros((self.nfields, self.K * self.Np))
+
+    def plane_wave(self, r, k, amplitude, rho, lam, mu, time=0.0) -> np.ndarray:
+        q = self.empty_fields()
+        kv = np.zeros(3)
+        kv[:len(k)] = k
+        lib().bfam_b200_init_plane_wave(self._ptr, _dp(np.ascontiguousarray(r)), _dp(kv),
+                                        amplitude, rho, lam, mu, time, _ptrs(list(q)))
+        return q
+
+    def gaussian_pulse(self, r, center, width) -> np.ndarray:
+        q = self.empty_fields()
+        c = np.zeros(3)
+        c[:len(center)] = center
+        lib().bfam_b200_init_gaussian_pulse(self._ptr, _dp(np.ascontiguousarray(r)), _dp(c),
+                                            width, _ptrs(list(q)))
+        return q
+
+
+def material_random(K: int, seed: int, rho=(1.0, 3.0), cp=(4.0, 6.0), ratio=(1.6, 2.0)):
+    """rho ~ U[rho], cp ~ U[cp], cs = cp / U[ratio] per element -> rho, lambda, mu."""
+    r, la, mu = np.zeros(K), np.zeros(K), np.zeros(K)
+    lib().bfam_b200_material_random(K, seed, rho[0], rho[1], cp[0], cp[1], ratio[0],
+                                    ratio[1], _dp(r), _dp(la), _dp(mu))
+    return r, la, mu
+
+
+# --------------------------------------------------------------- device layer
+
+class GpuDomain:
+    """A bfam_gpu_domain_t built from a Mesh's arrays (what an application
+    would pass from its bfam_subdomain_dgx_t and glue grid)."""
+
+    def __init__(self, mesh: Mesh, rho, lam, mu, flux: int = FLUX_UPWIND,
+                 precision: int = PRECISION_FP64, mem_budget_bytes: int = 0,
+                 device: int = 0):
+        L = lib()
+        self.mesh = mesh
+        N = mesh.N
+        self.r, self.w, self.wi, self.Dr = lgl_operators(N)
+        ops = mortar_operators(N, N)
+        self._keep = []
+        self.rho = np.ascontiguousarray(np.broadcast_to(rho, (mesh.K,)), dtype=np.float64)
+        self.lam = np.ascontiguousarray(np.broadcast_to(lam, (mesh.K,)), dtype=np.float64)
+        self.mu = np.ascontiguousarray(np.broadcast_to(mu, (mesh.K,)), dtype=np.float64)
+        vol = VolumeDesc()
+        vol.dim, vol.N, vol.K = mesh.dim, N, mesh.K
+        vol.r, vol.w, vol.Dr = _dp(self.r), _dp(self.w), _dp(self.Dr)
+        vol.vmapM = mesh.vmapM.ctypes.data_as(i32p)
+        vol.vmapP = mesh.vmapP.ctypes.data_as(i32p)
+        x0 = np.ascontiguousarray(mesh.x0)
+        hh = np.ascontiguousarray(mesh.h)
+        self._keep += [x0, hh, ops]
+        vol.x0, vol.h = _dp(x0), _dp(hh)
+        vol.rho, vol.lambda_, vol.mu = _dp(self.rho), _dp(self.lam), _dp(self.mu)
+        glue = GlueDesc()
+        glue.K = mesh.Kg
+        if mesh.Kg:
+            glue.EToEp = mesh.EToEp.ctypes.data_as(i32p)
+            glue.EToHp = mesh.EToHp.ctypes.data_as(i8p)
+            glue.EToOp = mesh.EToOp.ctypes.data_as(i8p)
+            glue.EToEm = mesh.EToEm.ctypes.data_as(i32p)
+            glue.EToFm = mesh.EToFm.ctypes.data_as(i8p)
+            glue.EToHm = mesh.EToHm.ctypes.data_as(i8p)
+            # interpolation = {same, r2b, r2t}; projection = {same, cfb, cft}
+            for slot, k in enumerate((0, 3, 4)):
+                glue.interpolation[slot] = _dp(ops[k]) if k else dp()
+            for slot, k in enumerate((0, 1, 2)):
+                glue.projection[slot] = _dp(ops[k]) if k else dp()
+        opt = Options()
+        opt.flux, opt.precision = flux, precision
+        opt.mem_budget_bytes, opt.device = mem_budget_bytes, device
+        h = C.c_void_p()
+        _check(L.bfam_gpu_domain_create(C.byref(vol), C.byref(glue), C.byref(opt),
+                                        C.byref(h)))
+        self._h = h
+        self.nfields = L.bfam_gpu_domain_num_fields(h)
+        self.field_length = L.bfam_gpu_domain_field_length(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().bfam_gpu_domain_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def device_bytes(self) -> int:
+        return int(lib().bfam_gpu_domain_device_bytes(self._h))
+
+    def set_fields(self, q: np.ndarray) -> None:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        assert q.shape == (self.nfields, self.field_length)
+        _check(lib().bfam_gpu_domain_set_fields(self._h, _ptrs(list(q))))
+
+    def get_fields(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.nfields, self.field_length))
+        _check(lib().bfam_gpu_domain_get_fields(self._h, _ptrs(list(out))))
+        return out
+
+    def rhs(self) -> np.ndarray:
+        out = np.empty((self.nfields, self.field_length))
+        _check(lib().bfam_gpu_domain_rhs(self._h, _ptrs(list(out))))
+        return out
+
+    def energy(self) -> float:
+        e = C.c_double()
+        _check(lib().bfam_gpu_domain_energy(self._h, C.byref(e)))
+        return e.value
+
+    def sync(self) -> None:
+        _check(lib().bfam_gpu_domain_sync(self._h))
+
+    def field_device_ptr(self, f: int) -> int:
+        return int(lib().bfam_gpu_domain_field_device_ptr(self._h, f) or 0)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().bfam_gpu_domain_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+
+class LSRK:
+    """bfam_ts_lsrk_t over a GpuDomain."""
+
+    def __init__(self, dom: GpuDomain, method: int = LSRK_KC54, t0: float = 0.0):
+        self.dom = dom
+        h = C.c_void_p()
+        _check(lib().bfam_ts_lsrk_init(C.byref(h), dom.handle, method, t0))
+        self._h = h
+
+    def step(self, dt: float, nsteps: int = 1, use_graph: bool = False) -> None:
+        _check(lib().bfam_ts_lsrk_step(self._h, dt, nsteps, 1 if use_graph else 0))
+
+    @property
+    def time(self) -> float:
+        t = C.c_double()
+        _check(lib().bfam_ts_lsrk_time(self._h, C.byref(t)))
+        return t.value
+
+    def free(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().bfam_ts_lsrk_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

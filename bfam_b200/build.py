@@ -1,0 +1,90 @@
+"""Build recipe for the in-tree shared libraries.
+
+    python -m bfam_b200.build            # product library + oracle
+    python -m bfam_b200.build --product  # product library only
+
+Products:
+  bfam_b200/libbfam_b200.so  -- CUDA kernels for sm_100a, the bfam_gpu C-ABI
+                                and the host front end (mesher, operators)
+  oracle/liboracle.so        -- the CPU oracle (test infrastructure)
+  oracle/_ref/*.so           -- the reference's own setup numerics compiled
+                                from its source (only where it is present)
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "bfam_b200"
+CSRC = PKG / "csrc"
+LIB = PKG / "libbfam_b200.so"
+ORACLE_LIB = ROOT / "oracle" / "liboracle.so"
+
+NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def _sources() -> list[Path]:
+    return [CSRC / "bfam_gpu.cu"] + sorted((CSRC / "host").glob("*.c"))
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in deps)
+
+
+def build_product(force: bool = False, verbose: bool = False) -> Path:
+    deps = _sources() + sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h"))
+    if not force and not _stale(LIB, deps):
+        return LIB
+    cmd = [
+        _nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17",
+        "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+        "--expt-relaxed-constexpr",
+        "-I", str(ROOT / "include"), "-I", str(CSRC),
+        "-o", str(LIB), *map(str, _sources()),
+    ]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_oracle(force: bool = False) -> Path:
+    src = ROOT / "oracle" / "dg_oracle.c"
+    if force or _stale(ORACLE_LIB, [src]):
+        subprocess.run(
+            ["gcc", "-std=gnu99", "-O2", "-fopenmp", "-fPIC", "-shared",
+             "-o", str(ORACLE_LIB), str(src), "-lm"],
+            check=True,
+        )
+    script = ROOT / "oracle" / "build_ref.sh"
+    if Path("/root/reference/src/bfam.c").exists() or os.environ.get("BFAM_REFERENCE_DIR"):
+        subprocess.run(["bash", str(script)], check=True)
+    return ORACLE_LIB
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--product", action="store_true")
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args(argv)
+    build_product(force=a.force, verbose=a.verbose)
+    if not a.product:
+        build_oracle(force=a.force)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,836 @@
+// C-ABI of the B200 device layer (declared in include/bfam_gpu.h).
+//
+// Host side: validates the bfam arrays handed over, turns vmapP and the
+// glue grid into compact per-element neighbour tables, uploads geometry,
+// material and operators, owns the device state and launches the fused
+// stage kernel once per LSRK stage (optionally replayed from a CUDA graph).
+#include "bfam_gpu.h"
+#include "dg_kernels.cuh"
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace bfam_b200;
+
+namespace
+{
+
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const char *fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                         \
+  do                                                                           \
+  {                                                                            \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      return fail(BFAM_GPU_ECUDA, "%s: %s (%s:%d)", #call,                     \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                 \
+  } while (0)
+
+typedef void (*stage_fn)(DomainView, StageParams);
+typedef void (*energy_fn)(const double *, size_t, const ElemData *,
+                          const double *, double *);
+
+struct KernelSet
+{
+  stage_fn stage = nullptr;
+  stage_fn rhs = nullptr;
+  energy_fn energy = nullptr;
+  int NT = 0;
+  size_t smem = 0;
+};
+
+template <int DIM, int N> KernelSet make_set()
+{
+  using S = Shape<DIM, N>;
+  KernelSet k;
+  k.stage = dg_stage_kernel<DIM, N, MODE_STAGE>;
+  k.rhs = dg_stage_kernel<DIM, N, MODE_RHS>;
+  k.energy = dg_energy_kernel<DIM, N>;
+  k.NT = S::NT;
+  k.smem = (size_t)S::SM_TOTAL * sizeof(double);
+  return k;
+}
+
+bool kernel_set(int dim, int N, KernelSet *out)
+{
+#define BFAM_CASE(D, NN)                                                       \
+  if (dim == D && N == NN)                                                     \
+  {                                                                            \
+    *out = make_set<D, NN>();                                                  \
+    return true;                                                               \
+  }
+  BFAM_CASE(2, 1) BFAM_CASE(2, 2) BFAM_CASE(2, 3) BFAM_CASE(2, 4)
+  BFAM_CASE(2, 5) BFAM_CASE(2, 6) BFAM_CASE(2, 7) BFAM_CASE(2, 8)
+  BFAM_CASE(3, 1) BFAM_CASE(3, 2) BFAM_CASE(3, 3) BFAM_CASE(3, 4)
+  BFAM_CASE(3, 5) BFAM_CASE(3, 6) BFAM_CASE(3, 7)
+#undef BFAM_CASE
+  return false;
+}
+
+int gmask_host(int dim, int Nq, int f, int pn)
+{
+  const int N = Nq - 1;
+  if (dim == 2)
+  {
+    switch (f)
+    {
+    case 0: return pn * Nq;
+    case 1: return pn * Nq + N;
+    case 2: return pn;
+    default: return N * Nq + pn;
+    }
+  }
+  const int a = pn % Nq, b = pn / Nq;
+  switch (f)
+  {
+  case 0: return Nq * a + Nq * Nq * b;
+  case 1: return N + Nq * a + Nq * Nq * b;
+  case 2: return a + Nq * Nq * b;
+  case 3: return a + Nq * N + Nq * Nq * b;
+  case 4: return a + Nq * b;
+  default: return a + Nq * b + Nq * Nq * N;
+  }
+}
+
+int face_perm_host(int dim, int Nq, int ns, int pn)
+{
+  const int N = Nq - 1;
+  if (dim == 2)
+    return ns ? N - pn : pn;
+  const int i = pn % Nq, j = pn / Nq, ir = N - i, jr = N - j;
+  switch (ns)
+  {
+  case 0: return i + j * Nq;
+  case 1: return j + i * Nq;
+  case 2: return ir + j * Nq;
+  case 3: return jr + i * Nq;
+  case 4: return j + ir * Nq;
+  case 5: return i + jr * Nq;
+  case 6: return jr + ir * Nq;
+  default: return ir + jr * Nq;
+  }
+}
+
+} // namespace
+
+struct bfam_gpu_domain
+{
+  int dim = 0, N = 0, Nq = 0, Np = 0, Nfp = 0, NF = 0, NFLD = 0;
+  int32_t K = 0, Kg = 0;
+  int device = 0;
+  int flux = 0, precision = 0;
+  size_t fs = 0;
+  KernelSet ks;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double *q[2] = {nullptr, nullptr};
+  double *dq = nullptr;
+  double *rhs = nullptr;
+  double *energy = nullptr;
+  ElemData *ed = nullptr;
+  int32_t *nbr = nullptr;
+  int8_t *nbrf = nullptr;
+  int32_t *gEm = nullptr, *gEp = nullptr;
+  int8_t *gFm = nullptr, *gHm = nullptr, *gOp = nullptr;
+  double *ops = nullptr;
+  int *err = nullptr;
+  int cur = 0;
+  size_t bytes = 0, budget = 0;
+  std::vector<void *> allocs;
+};
+
+struct bfam_ts_lsrk
+{
+  bfam_gpu_domain_t *dom = nullptr;
+  int ns = 0;
+  double A[6] = {0}, B[6] = {0}, C[7] = {0};
+  double t = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt[2] = {0, 0};
+};
+
+namespace
+{
+
+int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes)
+{
+  bytes = bytes ? bytes : 16;
+  if (d->budget && d->bytes + bytes > d->budget)
+    return fail(BFAM_GPU_ENOMEM,
+                "device budget exceeded: %zu + %zu bytes > budget %zu",
+                d->bytes, bytes, d->budget);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError();
+    return fail(BFAM_GPU_ENOMEM, "cudaMalloc(%zu): %s", bytes,
+                cudaGetErrorString(e));
+  }
+  d->allocs.push_back(*p);
+  d->bytes += bytes;
+  return 0;
+}
+
+template <typename T>
+int upload(bfam_gpu_domain_t *d, T **dst, const T *src, size_t n)
+{
+  int rc = dev_alloc(d, (void **)dst, n * sizeof(T));
+  if (rc)
+    return rc;
+  if (n)
+    CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+void release(bfam_gpu_domain_t *d)
+{
+  if (!d)
+    return;
+  cudaSetDevice(d->device);
+  for (void *p : d->allocs)
+    cudaFree(p);
+  d->allocs.clear();
+  if (d->own_stream && d->stream)
+    cudaStreamDestroy(d->stream);
+  delete d;
+}
+
+DomainView view(bfam_gpu_domain_t *d, int in)
+{
+  DomainView v;
+  v.K = d->K;
+  v.fs = d->fs;
+  v.qin = d->q[in];
+  v.qout = d->q[in ^ 1];
+  v.dq = d->dq;
+  v.rhs = d->rhs;
+  v.ed = d->ed;
+  v.nbr = d->nbr;
+  v.nbrf = d->nbrf;
+  v.gEm = d->gEm;
+  v.gEp = d->gEp;
+  v.gFm = d->gFm;
+  v.gHm = d->gHm;
+  v.gOp = d->gOp;
+  v.ops = d->ops;
+  v.err = d->err;
+  return v;
+}
+
+int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double dt,
+                 int first, int mode)
+{
+  StageParams sp;
+  sp.A = A;
+  sp.B = B;
+  sp.dt = dt;
+  sp.first_stage = first;
+  sp.flux = d->flux;
+  DomainView v = view(d, in);
+  stage_fn fn = mode == MODE_STAGE ? d->ks.stage : d->ks.rhs;
+  fn<<<d->K, d->ks.NT, d->ks.smem, d->stream>>>(v, sp);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int bfam_gpu_last_error(char *buf, size_t len)
+{
+  if (buf && len)
+  {
+    strncpy(buf, g_err.c_str(), len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)g_err.size();
+}
+
+uint64_t bfam_gpu_launch_count(void) { return g_launches.load(); }
+
+int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
+                           const bfam_gpu_glue_t *glue,
+                           const bfam_gpu_options_t *opts,
+                           bfam_gpu_domain_t **out)
+{
+  if (!out)
+    return fail(BFAM_GPU_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!vol || !opts)
+    return fail(BFAM_GPU_EINVAL, "vol/opts is NULL");
+  const int dim = vol->dim, N = vol->N;
+  if (dim != 2 && dim != 3)
+    return fail(BFAM_GPU_EINVAL, "dim must be 2 or 3 (got %d)", dim);
+  if (vol->K <= 0)
+    return fail(BFAM_GPU_EINVAL, "K must be positive (got %d)", vol->K);
+  KernelSet ks;
+  if (!kernel_set(dim, N, &ks))
+    return fail(BFAM_GPU_EUNSUPPORTED, "order N=%d in %dD is not compiled in",
+                N, dim);
+  if (!vol->r || !vol->w || !vol->Dr || !vol->vmapM || !vol->vmapP ||
+      !vol->x0 || !vol->h || !vol->rho || !vol->lambda || !vol->mu)
+    return fail(BFAM_GPU_EINVAL, "a required volume array is NULL");
+  if (opts->flux != BFAM_GPU_FLUX_UPWIND && opts->flux != BFAM_GPU_FLUX_CENTRAL)
+    return fail(BFAM_GPU_EINVAL, "unknown flux %d", opts->flux);
+  if (opts->precision != BFAM_GPU_PRECISION_FP64)
+    return fail(BFAM_GPU_EUNSUPPORTED, "precision %d is not available",
+                opts->precision);
+
+  const int Nq = N + 1;
+  const int Np = dim == 3 ? Nq * Nq * Nq : Nq * Nq;
+  const int Nfp = dim == 3 ? Nq * Nq : Nq;
+  const int NF = 2 * dim;
+  const int NFLD = dim == 3 ? 9 : 5;
+  const int32_t K = vol->K;
+  if ((int64_t)K * Np > INT32_MAX)
+    return fail(BFAM_GPU_EINVAL, "K*Np exceeds the int32 node index range");
+  const int nperm = dim == 3 ? 8 : 2;
+
+  // ---- vmapM must be bfam's canonical face mask layout
+  const size_t nmap = (size_t)K * NF * Nfp;
+  for (int32_t e = 0; e < K; ++e)
+    for (int f = 0; f < NF; ++f)
+      for (int pn = 0; pn < Nfp; ++pn)
+      {
+        const size_t id = ((size_t)e * NF + f) * Nfp + pn;
+        if (vol->vmapM[id] != e * Np + gmask_host(dim, Nq, f, pn))
+          return fail(BFAM_GPU_EINVAL,
+                      "vmapM[%zu] = %d is not element %d face %d node %d",
+                      id, vol->vmapM[id], e, f, pn);
+      }
+
+  // ---- vmapP -> (neighbour, face, permutation) or glue face
+  std::vector<int32_t> nbr((size_t)K * NF);
+  std::vector<int8_t> nbrf((size_t)K * NF, 0);
+  for (int32_t e = 0; e < K; ++e)
+    for (int f = 0; f < NF; ++f)
+    {
+      const int32_t *P = vol->vmapP + ((size_t)e * NF + f) * Nfp;
+      const int32_t *M = vol->vmapM + ((size_t)e * NF + f) * Nfp;
+      bool self = true;
+      for (int pn = 0; pn < Nfp && self; ++pn)
+        self = P[pn] == M[pn];
+      if (self)
+      {
+        nbr[(size_t)e * NF + f] = INT32_MIN; // filled from the glue grid
+        continue;
+      }
+      if (P[0] < 0 || P[0] >= K * Np)
+        return fail(BFAM_GPU_EINVAL, "vmapP out of range at element %d face %d",
+                    e, f);
+      const int32_t nb = P[0] / Np;
+      bool found = false;
+      for (int fn = 0; fn < NF && !found; ++fn)
+        for (int ns = 0; ns < nperm && !found; ++ns)
+        {
+          bool ok = true;
+          for (int pn = 0; pn < Nfp && ok; ++pn)
+            ok = P[pn] ==
+                 nb * Np + gmask_host(dim, Nq, fn, face_perm_host(dim, Nq, ns, pn));
+          if (ok)
+          {
+            found = true;
+            nbr[(size_t)e * NF + f] = nb;
+            nbrf[(size_t)e * NF + f] = (int8_t)(fn + NF * ns);
+          }
+        }
+      if (!found)
+        return fail(BFAM_GPU_EINVAL,
+                    "vmapP of element %d face %d is not a face of element %d "
+                    "under any orientation",
+                    e, f, nb);
+    }
+
+  // ---- glue grid
+  const int32_t Kg = glue ? glue->K : 0;
+  const int NPc = dim == 3 ? 4 : 2;
+  if (Kg < 0)
+    return fail(BFAM_GPU_EINVAL, "glue K is negative");
+  if (Kg > 0 && (!glue->EToEp || !glue->EToHp || !glue->EToOp ||
+                 !glue->EToEm || !glue->EToFm || !glue->EToHm))
+    return fail(BFAM_GPU_EINVAL, "a required glue array is NULL");
+  for (int32_t g = 0; g < Kg;)
+  {
+    const int32_t e = glue->EToEm[g];
+    const int f = glue->EToFm[g];
+    const int h = glue->EToHm[g];
+    if (e < 0 || e >= K || f < 0 || f >= NF || h < 0 || h > NPc)
+      return fail(BFAM_GPU_EINVAL, "glue element %d has bad (E, F, H) = "
+                  "(%d, %d, %d)", g, e, f, h);
+    if (nbr[(size_t)e * NF + f] != INT32_MIN)
+      return fail(BFAM_GPU_EINVAL,
+                  "glue element %d sits on element %d face %d whose vmapP "
+                  "does not point to itself",
+                  g, e, f);
+    const int cnt = h == 0 ? 1 : NPc;
+    if (g + cnt > Kg)
+      return fail(BFAM_GPU_EINVAL, "glue grid ends inside a hanging face");
+    for (int p = 0; p < cnt; ++p)
+    {
+      const int32_t gg = g + p;
+      if (glue->EToEm[gg] != e || glue->EToFm[gg] != f ||
+          glue->EToHm[gg] != (h == 0 ? 0 : p + 1))
+        return fail(BFAM_GPU_EINVAL,
+                    "glue elements of element %d face %d are not in receive "
+                    "order (element, face, hanging number)",
+                    e, f);
+      const int32_t pg = glue->EToEp[gg];
+      if (pg < 0 || pg >= Kg || glue->EToEp[pg] != gg)
+        return fail(BFAM_GPU_EINVAL,
+                    "glue EToEp is not an involution at %d (local glue grid)",
+                    gg);
+      if (glue->EToHp[gg] != glue->EToHm[pg])
+        return fail(BFAM_GPU_EINVAL, "glue EToHp[%d] disagrees with the "
+                    "partner's EToHm", gg);
+      if (glue->EToHm[gg] > 0 && glue->EToHm[pg] != 0)
+        return fail(BFAM_GPU_EINVAL, "hanging piece %d pairs with another "
+                    "hanging piece", gg);
+      if (glue->EToOp[gg] < 0 || glue->EToOp[gg] >= nperm)
+        return fail(BFAM_GPU_EINVAL, "glue orientation %d out of range",
+                    glue->EToOp[gg]);
+    }
+    nbr[(size_t)e * NF + f] = -1 - g;
+    g += cnt;
+  }
+  for (size_t i = 0; i < nbr.size(); ++i)
+    if (nbr[i] == INT32_MIN)
+      return fail(BFAM_GPU_EINVAL,
+                  "element %zu face %zu maps to itself but has no glue "
+                  "element",
+                  i / NF, i % NF);
+
+  // ---- operators: Dr | interp[3] | proj[3] | w
+  std::vector<double> ops(7 * Nq * Nq + Nq, 0.0);
+  std::memcpy(ops.data(), vol->Dr, sizeof(double) * Nq * Nq);
+  for (int k = 0; k < 6; ++k)
+  {
+    const double *src = nullptr;
+    if (glue && Kg > 0)
+      src = k < 3 ? glue->interpolation[k] : glue->projection[k - 3];
+    double *dst = ops.data() + (1 + k) * Nq * Nq;
+    if (src)
+      std::memcpy(dst, src, sizeof(double) * Nq * Nq);
+    else
+    {
+      if (Kg > 0 && (k % 3) != 0)
+        return fail(BFAM_GPU_EINVAL, "glue operator %s[%d] is NULL",
+                    k < 3 ? "interpolation" : "projection", k % 3);
+      for (int i = 0; i < Nq; ++i)
+        dst[i + Nq * i] = 1.0;
+    }
+    if ((k % 3) == 0 && src)
+      for (int i = 0; i < Nq * Nq; ++i)
+        if (std::fabs(dst[i] - ((i % (Nq + 1)) == 0 ? 1.0 : 0.0)) > 1e-12)
+          return fail(BFAM_GPU_EUNSUPPORTED,
+                      "non-identity same-level operator (glue order differs "
+                      "from the volume order) is not supported");
+  }
+  std::memcpy(ops.data() + 7 * Nq * Nq, vol->w, sizeof(double) * Nq);
+
+  // ---- per-element geometry and material
+  std::vector<ElemData> ed(K);
+  for (int32_t e = 0; e < K; ++e)
+  {
+    const double rho = vol->rho[e], la = vol->lambda[e], mu = vol->mu[e];
+    if (!(rho > 0) || !(mu > 0) || !(la + 2 * mu > 0))
+      return fail(BFAM_GPU_EINVAL,
+                  "element %d: need rho > 0, mu > 0, lambda + 2 mu > 0", e);
+    ElemData &x = ed[e];
+    x.irho = 1.0 / rho;
+    x.lam = la;
+    x.mu = mu;
+    x.Zp = std::sqrt(rho * (la + 2 * mu));
+    x.Zs = std::sqrt(rho * mu);
+    for (int a = 0; a < 3; ++a)
+    {
+      const double h = a < dim ? vol->h[3 * e + a] : 1.0;
+      if (!(h > 0))
+        return fail(BFAM_GPU_EINVAL, "element %d has edge %d <= 0", e, a);
+      (&x.rx)[a] = 2.0 / h;
+    }
+  }
+
+  // ---- device
+  bfam_gpu_domain_t *d = new bfam_gpu_domain_t();
+  d->dim = dim;
+  d->N = N;
+  d->Nq = Nq;
+  d->Np = Np;
+  d->Nfp = Nfp;
+  d->NF = NF;
+  d->NFLD = NFLD;
+  d->K = K;
+  d->Kg = Kg;
+  d->fs = (size_t)K * Np;
+  d->ks = ks;
+  d->flux = opts->flux;
+  d->precision = opts->precision;
+  d->device = opts->device;
+  d->budget = opts->mem_budget_bytes;
+  int rc = 0;
+#define TRY(x)                                                                 \
+  do                                                                           \
+  {                                                                            \
+    rc = (x);                                                                  \
+    if (rc)                                                                    \
+    {                                                                          \
+      release(d);                                                              \
+      return rc;                                                               \
+    }                                                                          \
+  } while (0)
+  {
+    cudaError_t ce = cudaSetDevice(opts->device);
+    if (ce != cudaSuccess)
+    {
+      release(d);
+      return fail(BFAM_GPU_ECUDA, "cudaSetDevice(%d): %s", opts->device,
+                  cudaGetErrorString(ce));
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && !d->budget)
+      d->budget = free_b;
+    ce = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess)
+    {
+      release(d);
+      return fail(BFAM_GPU_ECUDA, "stream: %s", cudaGetErrorString(ce));
+    }
+    d->own_stream = true;
+    for (stage_fn fn : {ks.stage, ks.rhs})
+    {
+      ce = cudaFuncSetAttribute((const void *)fn,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ks.smem);
+      if (ce != cudaSuccess)
+      {
+        release(d);
+        return fail(BFAM_GPU_ECUDA, "smem attribute: %s",
+                    cudaGetErrorString(ce));
+      }
+    }
+  }
+  const size_t state = (size_t)NFLD * d->fs * sizeof(double);
+  TRY(dev_alloc(d, (void **)&d->q[0], state));
+  TRY(dev_alloc(d, (void **)&d->q[1], state));
+  TRY(dev_alloc(d, (void **)&d->dq, state));
+  TRY(upload(d, &d->ed, ed.data(), ed.size()));
+  TRY(upload(d, &d->nbr, nbr.data(), nbr.size()));
+  TRY(upload(d, &d->nbrf, nbrf.data(), nbrf.size()));
+  TRY(upload(d, &d->ops, ops.data(), ops.size()));
+  if (Kg > 0)
+  {
+    TRY(upload(d, &d->gEm, glue->EToEm, Kg));
+    TRY(upload(d, &d->gEp, glue->EToEp, Kg));
+    TRY(upload(d, &d->gFm, glue->EToFm, Kg));
+    TRY(upload(d, &d->gHm, glue->EToHm, Kg));
+    TRY(upload(d, &d->gOp, glue->EToOp, Kg));
+  }
+  TRY(dev_alloc(d, (void **)&d->err, sizeof(int)));
+#undef TRY
+  if (cudaMemset(d->q[0], 0, state) != cudaSuccess ||
+      cudaMemset(d->q[1], 0, state) != cudaSuccess ||
+      cudaMemset(d->dq, 0, state) != cudaSuccess ||
+      cudaMemset(d->err, 0, sizeof(int)) != cudaSuccess)
+  {
+    release(d);
+    return fail(BFAM_GPU_ECUDA, "initial memset failed");
+  }
+  (void)nmap;
+  *out = d;
+  return 0;
+}
+
+int bfam_gpu_domain_free(bfam_gpu_domain_t *d)
+{
+  release(d);
+  return 0;
+}
+
+int bfam_gpu_domain_num_fields(const bfam_gpu_domain_t *d)
+{
+  return d ? d->NFLD : 0;
+}
+
+size_t bfam_gpu_domain_field_length(const bfam_gpu_domain_t *d)
+{
+  return d ? d->fs : 0;
+}
+
+size_t bfam_gpu_domain_device_bytes(const bfam_gpu_domain_t *d)
+{
+  return d ? d->bytes : 0;
+}
+
+int bfam_gpu_domain_set_stream(bfam_gpu_domain_t *d, void *stream)
+{
+  if (!d)
+    return fail(BFAM_GPU_EINVAL, "domain is NULL");
+  if (d->own_stream && d->stream)
+  {
+    cudaSetDevice(d->device);
+    cudaStreamDestroy(d->stream);
+  }
+  d->own_stream = false;
+  d->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int bfam_gpu_domain_sync(bfam_gpu_domain_t *d)
+{
+  if (!d)
+    return fail(BFAM_GPU_EINVAL, "domain is NULL");
+  CUDA_TRY(cudaSetDevice(d->device));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  int err = 0;
+  CUDA_TRY(cudaMemcpy(&err, d->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err)
+  {
+    CUDA_TRY(cudaMemset(d->err, 0, sizeof(int)));
+    return fail(BFAM_GPU_ETIMEOUT,
+                "a device-side wait on a bulk copy gave up (error flag %d)",
+                err);
+  }
+  return 0;
+}
+
+int bfam_gpu_domain_set_fields(bfam_gpu_domain_t *d,
+                               const double *const *fields)
+{
+  if (!d || !fields)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  for (int f = 0; f < d->NFLD; ++f)
+  {
+    if (!fields[f])
+      return fail(BFAM_GPU_EINVAL, "field %d is NULL", f);
+    CUDA_TRY(cudaMemcpyAsync(d->q[d->cur] + f * d->fs, fields[f],
+                             d->fs * sizeof(double), cudaMemcpyHostToDevice,
+                             d->stream));
+  }
+  return bfam_gpu_domain_sync(d);
+}
+
+int bfam_gpu_domain_get_fields(bfam_gpu_domain_t *d, double *const *fields)
+{
+  if (!d || !fields)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  for (int f = 0; f < d->NFLD; ++f)
+  {
+    if (!fields[f])
+      return fail(BFAM_GPU_EINVAL, "field %d is NULL", f);
+    CUDA_TRY(cudaMemcpyAsync(fields[f], d->q[d->cur] + f * d->fs,
+                             d->fs * sizeof(double), cudaMemcpyDeviceToHost,
+                             d->stream));
+  }
+  return bfam_gpu_domain_sync(d);
+}
+
+double *bfam_gpu_domain_field_device_ptr(bfam_gpu_domain_t *d, int f)
+{
+  if (!d || f < 0 || f >= d->NFLD)
+    return nullptr;
+  return d->q[d->cur] + f * d->fs;
+}
+
+int bfam_gpu_domain_rhs(bfam_gpu_domain_t *d, double *const *rhs)
+{
+  if (!d || !rhs)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  if (!d->rhs)
+  {
+    int rc = dev_alloc(d, (void **)&d->rhs,
+                       (size_t)d->NFLD * d->fs * sizeof(double));
+    if (rc)
+      return rc;
+  }
+  int rc = launch_stage(d, d->cur, 0.0, 0.0, 0.0, 1, MODE_RHS);
+  if (rc)
+    return rc;
+  for (int f = 0; f < d->NFLD; ++f)
+    CUDA_TRY(cudaMemcpyAsync(rhs[f], d->rhs + f * d->fs,
+                             d->fs * sizeof(double), cudaMemcpyDeviceToHost,
+                             d->stream));
+  return bfam_gpu_domain_sync(d);
+}
+
+int bfam_gpu_domain_energy(bfam_gpu_domain_t *d, double *energy)
+{
+  if (!d || !energy)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  if (!d->energy)
+  {
+    int rc = dev_alloc(d, (void **)&d->energy, (d->K + 1) * sizeof(double));
+    if (rc)
+      return rc;
+  }
+  d->ks.energy<<<d->K, d->ks.NT, 0, d->stream>>>(d->q[d->cur], d->fs, d->ed,
+                                                 d->ops, d->energy);
+  sum_kernel<<<1, 1024, 0, d->stream>>>(d->energy, d->K, d->energy + d->K);
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(energy, d->energy + d->K, sizeof(double),
+                           cudaMemcpyDeviceToHost, d->stream));
+  return bfam_gpu_domain_sync(d);
+}
+
+int bfam_ts_lsrk_init(bfam_ts_lsrk_t **ts, bfam_gpu_domain_t *dom, int method,
+                      double t0)
+{
+  if (!ts || !dom)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  *ts = nullptr;
+  bfam_ts_lsrk_t *s = new bfam_ts_lsrk_t();
+  s->dom = dom;
+  s->t = t0;
+  switch (method)
+  {
+  case 0: // KC54: Carpenter & Kennedy five-stage fourth-order
+    s->ns = 5;
+    s->A[0] = 0.0;
+    s->A[1] = (double)(-567301805773.0L / 1357537059087.0L);
+    s->A[2] = (double)(-2404267990393.0L / 2016746695238.0L);
+    s->A[3] = (double)(-3550918686646.0L / 2091501179385.0L);
+    s->A[4] = (double)(-1275806237668.0L / 842570457699.0L);
+    s->B[0] = (double)(1432997174477.0L / 9575080441755.0L);
+    s->B[1] = (double)(5161836677717.0L / 13612068292357.0L);
+    s->B[2] = (double)(1720146321549.0L / 2090206949498.0L);
+    s->B[3] = (double)(3134564353537.0L / 4481467310338.0L);
+    s->B[4] = (double)(2277821191437.0L / 14882151754819.0L);
+    s->C[0] = 0.0;
+    s->C[1] = (double)(1432997174477.0L / 9575080441755.0L);
+    s->C[2] = (double)(2526269341429.0L / 6820363962896.0L);
+    s->C[3] = (double)(2006345519317.0L / 3224310063776.0L);
+    s->C[4] = (double)(2802321613138.0L / 2924317926251.0L);
+    s->C[5] = 1.0;
+    break;
+  case 1: // forward Euler
+    s->ns = 1;
+    s->B[0] = 1.0;
+    s->C[1] = 1.0;
+    break;
+  case 2: // Heun
+    s->ns = 2;
+    s->A[1] = -1.0;
+    s->B[0] = 1.0;
+    s->B[1] = 0.5;
+    s->C[1] = 1.0;
+    s->C[2] = 1.0;
+    break;
+  case 3: // Williamson three-stage third-order
+    s->ns = 3;
+    s->A[1] = (double)(-5.0L / 9.0L);
+    s->A[2] = (double)(-153.0L / 128.0L);
+    s->B[0] = (double)(1.0L / 3.0L);
+    s->B[1] = (double)(15.0L / 16.0L);
+    s->B[2] = (double)(8.0L / 15.0L);
+    s->C[1] = (double)(1.0L / 3.0L);
+    s->C[2] = (double)(3.0L / 4.0L);
+    s->C[3] = 1.0;
+    break;
+  default:
+    delete s;
+    return fail(BFAM_GPU_EINVAL, "unknown LSRK method %d", method);
+  }
+  *ts = s;
+  return 0;
+}
+
+int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
+{
+  if (!ts || nsteps < 0)
+    return fail(BFAM_GPU_EINVAL, "bad arguments");
+  bfam_gpu_domain_t *d = ts->dom;
+  CUDA_TRY(cudaSetDevice(d->device));
+  for (int st = 0; st < nsteps; ++st)
+  {
+    const int c0 = d->cur;
+    if (use_graph && d->stream)
+    {
+      if (!ts->graph[c0] || ts->graph_dt[c0] != dt)
+      {
+        if (ts->graph[c0])
+          cudaGraphExecDestroy(ts->graph[c0]);
+        ts->graph[c0] = nullptr;
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(d->stream,
+                                        cudaStreamCaptureModeThreadLocal));
+        int in = c0, rc = 0;
+        for (int s = 0; s < ts->ns && !rc; ++s, in ^= 1)
+          rc = launch_stage(d, in, ts->A[s], ts->B[s], dt, s == 0, MODE_STAGE);
+        cudaError_t ce = cudaStreamEndCapture(d->stream, &g);
+        if (rc)
+          return rc;
+        if (ce != cudaSuccess)
+          return fail(BFAM_GPU_ECUDA, "graph capture: %s",
+                      cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&ts->graph[c0], g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess)
+          return fail(BFAM_GPU_ECUDA, "graph instantiate: %s",
+                      cudaGetErrorString(ce));
+        ts->graph_dt[c0] = dt;
+        // capture counted the launches once; replays are counted below
+        g_launches.fetch_sub(ts->ns, std::memory_order_relaxed);
+      }
+      CUDA_TRY(cudaGraphLaunch(ts->graph[c0], d->stream));
+      g_launches.fetch_add(ts->ns, std::memory_order_relaxed);
+    }
+    else
+    {
+      int in = c0;
+      for (int s = 0; s < ts->ns; ++s, in ^= 1)
+      {
+        int rc = launch_stage(d, in, ts->A[s], ts->B[s], dt, s == 0,
+                              MODE_STAGE);
+        if (rc)
+          return rc;
+      }
+    }
+    d->cur = (ts->ns & 1) ? c0 ^ 1 : c0;
+    ts->t += dt;
+  }
+  return 0;
+}
+
+int bfam_ts_lsrk_time(const bfam_ts_lsrk_t *ts, double *t)
+{
+  if (!ts || !t)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  *t = ts->t;
+  return 0;
+}
+
+int bfam_ts_lsrk_free(bfam_ts_lsrk_t *ts)
+{
+  if (!ts)
+    return 0;
+  for (int i = 0; i < 2; ++i)
+    if (ts->graph[i])
+      cudaGraphExecDestroy(ts->graph[i]);
+  delete ts;
+  return 0;
+}
+
+} // extern "C"

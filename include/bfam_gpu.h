@@ -1,0 +1,180 @@
+/*
+ * bfam_gpu.h -- the B200 device layer for bfam's DG elastic hot path.
+ *
+ * This is the drop-in boundary: plain C, plain pointers and sizes.  It takes
+ * the arrays an application already holds in bfam's structs and replaces the
+ * reference's OCCA device layer ("bfamo", src/bfam.c:8389-9091,
+ * src/bfam.h:1480-1864) for the elastic right-hand side and LSRK step:
+ *
+ *   reference (bfam)                               here
+ *   ----------------------------------------------------------------------
+ *   bfam_subdomain_dgx_t: N, K, Np, r, w, Dr,     bfam_gpu_volume_t
+ *     vmapM, vmapP (src/bfam.h:1364-1420)
+ *   bfam_subdomain_dgx_glue_data_t: EToEp, EToHp,  bfam_gpu_glue_t
+ *     EToOp, EToEm, EToFm, EToHm, mapOp,
+ *     interpolation[3], projection[3]
+ *     (src/bfam.h:1319-1362)
+ *   bfam_subdomain_dgx_field_add + field arrays    bfam_gpu_domain_set_fields
+ *     (src/bfam.c:6574-6597)                         / _get_fields
+ *   bfamo_device_malloc with memory budget         bfam_gpu_domain_create
+ *     (src/bfam.c:8561-8589)                         (opts.mem_budget_bytes)
+ *   bfamo_lsrk_t / bfamo_lsrk_init                 bfam_ts_lsrk_init
+ *     (src/bfam.h:1840-1863, src/bfam.c:8996-9090)
+ *   application stage kernels via BFAMO_KERNEL_RUN bfam_ts_lsrk_step
+ *     (src/bfam.h:1673-1717)
+ *   bfamo_communicator_post_* / *_wait             (none: neighbour traces
+ *     (src/bfam.c:8900-8930)                        are read on the device)
+ *
+ * Every function returns 0 on success and a negative BFAM_GPU_E* code on
+ * failure; bfam_gpu_last_error() gives the message.  The library never
+ * aborts the process.  One domain is not safe to use from two host threads
+ * at once.
+ */
+#ifndef BFAM_GPU_H
+#define BFAM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum
+{
+  BFAM_GPU_OK = 0,
+  BFAM_GPU_EINVAL = -1,   /* malformed input (sizes, maps, operators) */
+  BFAM_GPU_ENOMEM = -2,   /* device allocation failed or over budget */
+  BFAM_GPU_ECUDA = -3,    /* CUDA runtime error */
+  BFAM_GPU_ETIMEOUT = -4, /* a bounded device-side wait gave up */
+  BFAM_GPU_EUNSUPPORTED = -5 /* order / dimension not compiled in */
+};
+
+/* numerical flux */
+enum
+{
+  BFAM_GPU_FLUX_UPWIND = 0,
+  BFAM_GPU_FLUX_CENTRAL = 1
+};
+
+/* arithmetic of the right-hand side; state and LSRK stay FP64 either way */
+enum
+{
+  BFAM_GPU_PRECISION_FP64 = 0,
+  /* volume derivative, flux, lift and mortar interpolation in FP32; the
+   * mortar L2 projection, stage update and energy in FP64 */
+  BFAM_GPU_PRECISION_FP32 = 1
+};
+
+/* One dgx volume subdomain (bfam_subdomain_dgx_t) of an adapted Cartesian
+ * mesh.  Arrays are read during bfam_gpu_domain_create only. */
+typedef struct
+{
+  int dim;          /* 2 or 3 */
+  int N;            /* order; Nq = N+1 nodes per axis */
+  int32_t K;        /* elements */
+  const double *r;  /* Nq LGL nodes (bfam "r_N") */
+  const double *w;  /* Nq LGL weights ("w_N") */
+  const double *Dr; /* Nq*Nq differentiation matrix ("Dr_N"), column-major */
+  const int32_t *vmapM; /* K * 2dim * Nfp */
+  const int32_t *vmapP; /* K * 2dim * Nfp */
+  /* affine element geometry: lower corner and edge lengths, K*3 each */
+  const double *x0;
+  const double *h;
+  /* isotropic material per element */
+  const double *rho;
+  const double *lambda;
+  const double *mu;
+} bfam_gpu_volume_t;
+
+/* The local glue grid holding this subdomain's hanging faces
+ * (bfam_subdomain_dgx_glue_data_t; minus and plus side in one subdomain).
+ * K == 0 for a conforming mesh. */
+typedef struct
+{
+  int32_t K;
+  const int32_t *EToEp;
+  const int8_t *EToHp;
+  const int8_t *EToOp;
+  const int32_t *EToEm;
+  const int8_t *EToFm;
+  const int8_t *EToHm;
+  /* 1-D operators, Nq*Nq column-major; NULL means identity.
+   * interpolation: [same, refine-to-bottom, refine-to-top];
+   * projection:    [same, coarsen-from-bottom, coarsen-from-top] */
+  const double *interpolation[3];
+  const double *projection[3];
+} bfam_gpu_glue_t;
+
+typedef struct
+{
+  int flux;              /* BFAM_GPU_FLUX_* */
+  int precision;         /* BFAM_GPU_PRECISION_* */
+  size_t mem_budget_bytes; /* 0: no budget beyond the device's free memory */
+  int device;            /* CUDA device ordinal */
+} bfam_gpu_options_t;
+
+typedef struct bfam_gpu_domain bfam_gpu_domain_t;
+typedef struct bfam_ts_lsrk bfam_ts_lsrk_t;
+
+/* Validate vol/glue, derive the compact on-device neighbour tables from
+ * vmapP and the glue arrays, upload geometry, material and operators and
+ * allocate the state (q twice, dq).  Fields start at zero. */
+int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
+                           const bfam_gpu_glue_t *glue,
+                           const bfam_gpu_options_t *opts,
+                           bfam_gpu_domain_t **out);
+int bfam_gpu_domain_free(bfam_gpu_domain_t *dom);
+
+/* Number of fields (5 in 2D: vx vy sxx syy sxy; 9 in 3D: vx vy vz sxx syy
+ * szz sxy sxz syz) and their length K*Np. */
+int bfam_gpu_domain_num_fields(const bfam_gpu_domain_t *dom);
+size_t bfam_gpu_domain_field_length(const bfam_gpu_domain_t *dom);
+/* device bytes held by the domain */
+size_t bfam_gpu_domain_device_bytes(const bfam_gpu_domain_t *dom);
+
+/* Copy the state from / to bfam's per-field host arrays (fields[f] holds
+ * K*Np doubles, node fastest, element next). Synchronous. */
+int bfam_gpu_domain_set_fields(bfam_gpu_domain_t *dom,
+                               const double *const *fields);
+int bfam_gpu_domain_get_fields(bfam_gpu_domain_t *dom, double *const *fields);
+
+/* Evaluate the right-hand side of the current state into fields (host). */
+int bfam_gpu_domain_rhs(bfam_gpu_domain_t *dom, double *const *rhs);
+
+/* Discrete energy sum_e J_e sum_n w_n (rho|v|^2 + S:C^-1:S)/2 (FP64). */
+int bfam_gpu_domain_energy(bfam_gpu_domain_t *dom, double *energy);
+
+/* Device pointer of field f of the current state (for callers that keep
+ * inputs resident and time device work only). */
+double *bfam_gpu_domain_field_device_ptr(bfam_gpu_domain_t *dom, int f);
+
+/* Stream the domain launches on (cudaStream_t passed as void*; NULL is the
+ * legacy default stream). */
+int bfam_gpu_domain_set_stream(bfam_gpu_domain_t *dom, void *stream);
+
+/* LSRK stepper over a domain; method numbering follows bfamo_lsrk_method_t
+ * (0 KC54, 1 FE, 2 HEUN, 3 W33). */
+int bfam_ts_lsrk_init(bfam_ts_lsrk_t **ts, bfam_gpu_domain_t *dom, int method,
+                      double t0);
+/* Advance nsteps steps of size dt.  Asynchronous on the domain's stream;
+ * use_graph != 0 replays each step from a captured CUDA graph. */
+int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps,
+                      int use_graph);
+int bfam_ts_lsrk_time(const bfam_ts_lsrk_t *ts, double *t);
+int bfam_ts_lsrk_free(bfam_ts_lsrk_t *ts);
+
+/* Wait for the domain's stream and report device-side errors. */
+int bfam_gpu_domain_sync(bfam_gpu_domain_t *dom);
+
+/* Kernel launches issued by this library since process start. */
+uint64_t bfam_gpu_launch_count(void);
+
+/* Copy of the last error message of the calling thread (NUL-terminated,
+ * truncated to len). Returns the message length. */
+int bfam_gpu_last_error(char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,122 @@
+"""The C-ABI library loads, exports every declared symbol, and rejects
+malformed bfam arrays before touching the device."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import bfam_b200 as bf
+
+INCLUDE = Path(__file__).resolve().parent.parent / "include"
+
+
+def declared_functions():
+    names = []
+    for h in sorted(INCLUDE.glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(bfam_[A-Za-z0-9_]+)\s*\(", text):
+            names.append(m.group(1))
+    return sorted(set(names))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = C.CDLL(str(bf.LIB_PATH))
+    names = declared_functions()
+    assert len(names) > 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def _vol(m, ops_keep):
+    r, w, wi, D = bf.lgl_operators(m.N)
+    rho, lam, mu = (np.ones(m.K), np.full(m.K, 2.0), np.ones(m.K))
+    keep = [r, w, D, rho, lam, mu, np.ascontiguousarray(m.x0), np.ascontiguousarray(m.h)]
+    ops_keep.extend(keep)
+    v = bf.VolumeDesc()
+    v.dim, v.N, v.K = m.dim, m.N, m.K
+    v.r, v.w, v.Dr = (bf._dp(a) for a in (r, w, D))
+    v.vmapM = m.vmapM.ctypes.data_as(bf.i32p)
+    v.vmapP = m.vmapP.ctypes.data_as(bf.i32p)
+    v.x0, v.h = bf._dp(keep[6]), bf._dp(keep[7])
+    v.rho, v.lambda_, v.mu = bf._dp(rho), bf._dp(lam), bf._dp(mu)
+    return v
+
+
+def _create(v, g=None):
+    opt = bf.Options()
+    h = C.c_void_p()
+    rc = bf.lib().bfam_gpu_domain_create(C.byref(v), C.byref(g) if g else None,
+                                         C.byref(opt), C.byref(h))
+    return rc, h
+
+
+def test_rejects_corrupt_vmapP():
+    m = bf.Mesh(3, 2, (2, 2, 2))
+    keep = []
+    v = _vol(m, keep)
+    bad = m.vmapP.copy()
+    bad[5] = bad[6]  # not a face of any element under any orientation
+    v.vmapP = bad.ctypes.data_as(bf.i32p)
+    rc, _ = _create(v)
+    assert rc == -1 and "vmapP" in bf.last_error()
+
+
+def test_rejects_noncanonical_vmapM():
+    m = bf.Mesh(2, 2, (3, 3))
+    keep = []
+    v = _vol(m, keep)
+    bad = m.vmapM.copy()
+    bad[0] += 1
+    v.vmapM = bad.ctypes.data_as(bf.i32p)
+    rc, _ = _create(v)
+    assert rc == -1 and "vmapM" in bf.last_error()
+
+
+def test_rejects_missing_glue():
+    m = bf.Mesh(3, 2, (2, 2, 2), refine_prob=0.5, seed=1)
+    assert m.Kg > 0
+    keep = []
+    v = _vol(m, keep)
+    rc, _ = _create(v)  # hanging faces but no glue grid
+    assert rc == -1 and "glue" in bf.last_error()
+
+
+def test_rejects_broken_glue_involution():
+    m = bf.Mesh(3, 2, (2, 2, 2), refine_prob=0.5, seed=1)
+    keep = []
+    v = _vol(m, keep)
+    ops = bf.mortar_operators(2, 2)
+    g = bf.GlueDesc()
+    ep = m.EToEp.copy()
+    ep[0], ep[1] = ep[1], ep[0]
+    keep += [ep, ops]
+    g.K = m.Kg
+    g.EToEp = ep.ctypes.data_as(bf.i32p)
+    for name in ("EToHp", "EToOp", "EToFm", "EToHm"):
+        setattr(g, name, getattr(m, name).ctypes.data_as(bf.i8p))
+    g.EToEm = m.EToEm.ctypes.data_as(bf.i32p)
+    for s, k in enumerate((0, 3, 4)):
+        g.interpolation[s] = bf._dp(ops[k]) if k else bf.dp()
+    for s, k in enumerate((0, 1, 2)):
+        g.projection[s] = bf._dp(ops[k]) if k else bf.dp()
+    rc, _ = _create(v, g)
+    assert rc == -1 and ("involution" in bf.last_error() or "EToHp" in bf.last_error())
+
+
+def test_rejects_bad_material_and_order():
+    m = bf.Mesh(2, 2, (2, 2))
+    keep = []
+    v = _vol(m, keep)
+    mu0 = np.zeros(m.K)
+    keep.append(mu0)
+    v.mu = bf._dp(mu0)
+    rc, _ = _create(v)
+    assert rc == -1 and "mu" in bf.last_error()
+    v2 = _vol(bf.Mesh(3, 9, (1, 1, 1)), keep)
+    rc, _ = _create(v2)
+    assert rc == -5
