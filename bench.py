@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""Benchmark of the DG elastic RHS + LSRK hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config cfg1|cfg0|cfg2]
+
+Workload (default cfg1): 3D velocity-stress elasticity, 32^3 periodic brick,
+each base cell refined once with probability 0.3 (seed 0, 2:1 hanging faces
+through mortars), N=5, heterogeneous material, Gaussian pressure pulse; FP64
+state.  A step is one KC54 LSRK step (5 stages) over the whole mesh;
+DOF-updates = DOFs x stages.  Inputs (3.2 GB of state) exceed L2 (126 MB),
+so no flush is needed between steps.
+
+Metric: DOF-updates/s (higher is better).  `value` is device-timed with the
+state resident in HBM; `e2e` is one full solve through the C-ABI
+(bfam_gpu_domain_set_fields from pinned host memory, 200 steps,
+bfam_gpu_domain_get_fields back to the host).  Multi-GPU: independent
+replicas, one per rank (the path has no exchange step on one mesh).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+ALG_BYTES_PER_DOF_UPDATE = {5: 30.4}  # KC54: (24 + 4*32)/5 bytes, FP64 q and dq
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--graph", type=int, default=1)
+    return ap.parse_args()
+
+
+def build_problem(name):
+    from bfam_b200 import configs
+    return {"cfg0": configs.cfg0, "cfg1": configs.cfg1, "cfg2": configs.cfg2}[name]()
+
+
+def workload_desc(p):
+    m = p.mesh
+    return {
+        "workload": f"{p.name}: {m.dim}D elastic DG N={m.N}, "
+                    + ("x".join(str(x) for x in m.nbase[:m.dim]))
+                    + f" periodic brick, refine p={p.meta.get('refine_prob', 0.0)}, "
+                    f"K={m.K} elements, {m.Kg} glue elements, KC54 LSRK",
+        "dofs": int(m.ndof),
+        "elements": int(m.K),
+        "order": int(m.N),
+        "nsteps_solve": int(p.nsteps),
+        "l2_flush": "inputs larger than L2 (state %.2f GB)" % (3 * m.ndof * 8 / 1e9),
+    }
+
+
+def measured_peak():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel_key):
+    """dram bytes per launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel_key:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if r and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) > 1 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 4 + i and r[4 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_init():
+    import torch
+    import torch.distributed as dist
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1 and not dist.is_initialized():
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def cpu_baseline_sample(p, budget_s=12.0):
+    """The oracle (FP64 CPU restatement) on this host's cores: whole stages
+    (RHS + LSRK update) over the full mesh until budget_s elapses."""
+    from oracle import oracle as orc
+    o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
+    threads = orc.max_threads()
+    q = p.q0.copy()
+    t0 = time.perf_counter()
+    stages = 0
+    while True:
+        q = o.lsrk(q, p.dt, 1, nthreads=threads)
+        stages += 5
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": p.ndof * stages / el, "unit": "DOF-updates/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{stages // 5} KC54 step(s) = {stages} stages over the full "
+                      f"{p.name} mesh ({p.ndof} DOFs), {threads} threads, {el:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    p = build_problem(args.config)
+    from oracle import oracle as orc
+    o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
+    threads = orc.max_threads()
+    q = p.q0.copy()
+    # warm-up: one stage-equivalent; each timed step = one KC54 step
+    for _ in range(max(0, min(args.warmup, 1))):
+        q = o.lsrk(q, p.dt, 1, nthreads=threads)
+    steps = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        q = o.lsrk(q, p.dt, 1, nthreads=threads)
+    el = time.perf_counter() - t0
+    v = p.ndof * 5 * steps / el
+    line = {
+        "impl": "reference", "metric": "DOF-updates/s", "value": v, "unit": "DOF-updates/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_desc(p),
+        "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} KC54 step(s) over the full mesh (the reference "
+                                   "has no elastic RHS; this is the oracle's restatement)"},
+        "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    import bfam_b200 as bf
+
+    p = build_problem(args.config)
+    dom = bf.GpuDomain(p.mesh, p.rho, p.lam, p.mu, device=local)
+    stream = torch.cuda.Stream(device=local)
+    dom.set_stream(stream.cuda_stream)
+    dom.set_fields(p.q0)
+    ts = bf.LSRK(dom)
+    use_graph = bool(args.graph)
+    for _ in range(max(3, args.warmup)):
+        ts.step(p.dt, 1, use_graph=use_graph)
+    dom.sync()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    n0 = bf.launch_count()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        ts.step(p.dt, args.steps, use_graph=use_graph)
+        ev1.record(stream)
+        ev1.synchronize()
+    launches = bf.launch_count() - n0
+    dom.sync()
+    ms = ev0.elapsed_time(ev1)
+    t_local = ms / 1e3
+    if ws > 1:
+        t = torch.tensor([t_local], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t_max = float(t.item())
+    else:
+        t_max = t_local
+    ns = 5
+    dof_updates = p.ndof * ns * args.steps
+    value = dof_updates * ws / t_max
+
+    # roofline of the dominant (only) kernel: the fused stage kernel
+    n_launch = ns * args.steps
+    per_launch_s = t_local / n_launch
+    alg_bytes_per_launch = p.ndof * ALG_BYTES_PER_DOF_UPDATE[ns]
+    achieved = alg_bytes_per_launch / per_launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profiled_traffic(f"dg_stage_kernel_3d_N{p.mesh.N}") if p.mesh.dim == 3 else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"of {peak_kind}",
+                "traffic": traffic, "kernel": "dg_stage_kernel (fused volume+face+mortar+LSRK)",
+                "alg_bytes_per_launch": alg_bytes_per_launch}
+
+    # e2e: one full solve through the C-ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty((dom.nfields, dom.field_length), dtype=torch.float64,
+                           pin_memory=True)
+        host_np = host.numpy()
+        host_np[...] = p.q0
+        out = torch.empty_like(host, pin_memory=True).numpy()
+        tsolve = bf.LSRK(dom)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        dom.set_fields(host_np)
+        tsolve.step(p.dt, p.nsteps, use_graph=use_graph)
+        dom.get_fields(out)
+        e1.record(stream)
+        e1.synchronize()
+        el = e0.elapsed_time(e1) / 1e3
+        if ws > 1:
+            t = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            el = float(t.item())
+        nbytes = host_np.nbytes
+        e2e = {"value": p.ndof * ns * p.nsteps * ws / el, "unit": "DOF-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "step": f"one solve: upload state, {p.nsteps} LSRK steps, download state",
+               "seconds": el}
+        tsolve.free()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(p)
+
+    if rank == 0:
+        line = {
+            "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_desc(p), parallelism=f"replicas{ws}",
+                           cuda_graph=use_graph),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ts.free()
+    dom.free()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -83,7 +83,8 @@ template <int DIM, int N> struct Shape
   // shared memory in doubles
   static constexpr int SM_QS = NFLD * Np;
   static constexpr int SM_JF = NF * NJ * Nfp;
-  static constexpr int SM_MB = NFLD * Nfp;
+  // mortar buffers hold either NFLD traces or NJ jump components
+  static constexpr int SM_MB = (NFLD > NJ ? NFLD : NJ) * Nfp;
   static constexpr int SM_TOTAL = OPS_PAD + SM_QS + SM_JF + 3 * SM_MB + 2;
   static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
 };
