@@ -48,12 +48,16 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graph", type=int, default=1)
+    ap.add_argument("--n", type=int, default=32,
+                    help="base cells per axis for cfg1/cfg2 (smaller cases for profiling)")
     return ap.parse_args()
 
 
-def build_problem(name):
+def build_problem(name, n=32):
     from bfam_b200 import configs
-    return {"cfg0": configs.cfg0, "cfg1": configs.cfg1, "cfg2": configs.cfg2}[name]()
+    if name == "cfg0":
+        return configs.cfg0()
+    return {"cfg1": configs.cfg1, "cfg2": configs.cfg2}[name](n=n)
 
 
 def workload_desc(p):
@@ -182,7 +186,7 @@ def run_reference(args):
     ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return 0
-    p = build_problem(args.config)
+    p = build_problem(args.config, args.n)
     from oracle import oracle as orc
     o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
     threads = orc.max_threads()
@@ -221,7 +225,7 @@ def main():
     torch.cuda.set_device(local)
     import bfam_b200 as bf
 
-    p = build_problem(args.config)
+    p = build_problem(args.config, args.n)
     dom = bf.GpuDomain(p.mesh, p.rho, p.lam, p.mu, device=local)
     stream = torch.cuda.Stream(device=local)
     dom.set_stream(stream.cuda_stream)

@@ -1,21 +1,28 @@
 // Fused DG stage kernel for the isotropic velocity-stress elastic system on
 // affine Cartesian elements (sm_100a).
 //
-// One launch per LSRK stage does, per element:
-//   volume  : tensor-product LGL derivative along each axis from shared
-//             memory (the BFAM_KRON_* contractions, src/bfam.c:3137-3624);
-//   face    : upwind flux on neighbour traces gathered through the compact
-//             neighbour table (the on-device replacement of vmapP and of the
-//             bfam_communicator ghost exchange, src/bfam.c:6783-6877,
-//             2418-2679), lifted with the lumped LGL mass;
-//   mortar  : for faces that go through the glue grid (2:1 hanging faces,
-//             src/bfam.c:7328-7520) the traces are interpolated to each
-//             half-size mortar piece (interpolation[1..2]), the flux is
-//             evaluated there and L2-projected back (projection[1..2]);
+// One launch per LSRK stage does, per element (one CTA per element):
+//   gather  : every global read of the element is issued up front -- its own
+//             state q (and dq) by TMA bulk copies into shared memory, the
+//             neighbours' face traces by 8-byte cp.async gathers straight into
+//             shared memory.  This gather is the on-device replacement of
+//             vmapP and of the bfam_communicator ghost exchange
+//             (src/bfam.c:6783-6877, 2418-2679);
+//   face    : upwind flux on the gathered traces (conforming faces and the
+//             fine side of hanging faces);
+//   mortar  : faces that go through the glue grid (2:1 hanging faces,
+//             src/bfam.c:7328-7520): on the fine side the coarse neighbour's
+//             trace is interpolated to this element's mortar piece
+//             (interpolation[1..2]); on the coarse side the element's own trace
+//             is interpolated to the four (2D: two) pieces, the flux evaluated
+//             there against each fine neighbour and L2-projected back
+//             (projection[1..2]) -- all pieces of a face at once;
+//   volume  : tensor-product LGL derivative along each axis from shared memory
+//             (the BFAM_KRON_* contractions, src/bfam.c:3137-3624);
 //   update  : the 2N-storage LSRK stage dq = A dq + dt rhs, q' = q + B dq
-//             (bfamo_lsrk_t, src/bfam.h:1840-1846) in the tail, writing the
-//             new state to the other state buffer so that neighbours of
-//             every element read the stage input unchanged.
+//             (bfamo_lsrk_t, src/bfam.h:1840-1846) in the tail, writing the new
+//             state to the other state buffer so that every element's
+//             neighbours read the stage input unchanged.
 //
 // State layout in HBM: field-major, element, node (bfam's per-field arrays
 // stacked): q[f * K * Np + e * Np + n], n = i + Nq (j + Nq k).
@@ -72,21 +79,29 @@ template <int DIM, int N> struct Shape
   static constexpr int Nfp = DIM == 3 ? Nq * Nq : Nq;
   static constexpr int NF = 2 * DIM;
   static constexpr int NFLD = DIM == 3 ? 9 : 5;
-  static constexpr int NJ = 6; // (T* - T-, v* - v-), 3 components each
-  static constexpr int NP = DIM == 3 ? 4 : 2; // mortar pieces per coarse face
+  // stored jump components: (T* - T-)[0..DIM), (v* - v-)[0..DIM)
+  static constexpr int NJ = 2 * DIM;
+  static constexpr int NPC = DIM == 3 ? 4 : 2; // mortar pieces per coarse face
+  static constexpr int ROWS = DIM == 3 ? Nq : 1; // rows of a face
   static constexpr int work = (Np > NF * Nfp ? Np : NF * Nfp);
   static constexpr int NT = ((work + 31) / 32) * 32 > 1024
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
+  // CTAs per SM the register allocation is sized for (about 96 registers)
+  static constexpr int MINB_RAW = 65536 / (NT * 96);
+  static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW);
   static constexpr int OPS = 7 * Nq * Nq + Nq;
   static constexpr int OPS_PAD = (OPS + 1) & ~1; // keep 16-byte alignment
-  // shared memory in doubles
-  static constexpr int SM_QS = NFLD * Np;
-  static constexpr int SM_JF = NF * NJ * Nfp;
-  // mortar buffers hold either NFLD traces or NJ jump components
-  static constexpr int SM_MB = (NFLD > NJ ? NFLD : NJ) * Nfp;
-  static constexpr int SM_TOTAL = OPS_PAD + SM_QS + SM_JF + 3 * SM_MB + 2;
-  static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
+  static constexpr bool TMA = (Np % 2) == 0;     // 16-byte aligned element rows
+  static constexpr bool DQ_SMEM = NFLD * Np * 8 <= 20 * 1024;
+  // shared memory regions in doubles (all even, so 16-byte aligned)
+  static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2;
+  static constexpr int SM_DQ = DQ_SMEM ? SM_QS : 0;
+  static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
+  static constexpr int SM_OI = NPC * NFLD * Nfp + (NPC * NFLD * Nfp) % 2;
+  static constexpr int SM_FC = 4 * (NF + NPC);
+  static constexpr int SM_TOTAL =
+      OPS_PAD + SM_QS + SM_DQ + SM_PT + 2 * SM_OI + SM_FC + 4;
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -120,6 +135,24 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
                "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
+}
+
+// 8-byte asynchronous gather global -> shared (completes with the group)
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)),
+               "l"(src)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int NPENDING> __device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;" ::"n"(NPENDING) : "memory");
 }
 
 __device__ __forceinline__ uint64_t global_ns()
@@ -223,123 +256,138 @@ template <int DIM, int N> __device__ __forceinline__ int map_op(int o, int pn)
 
 // ------------------------------------------------------------- physics
 
-// Jump terms (T* - T-, v* - v-) at one face point.  qm/qp hold the point's
-// fields (velocity then stress, bfam field order); nx,ny,nz is the minus
-// side's outward unit normal.  Upwind: exact Riemann solution of the normal
-// (P, impedance Zp) and tangential (S, impedance Zs) problems; T - Z v
-// travels out of the minus side, T + Z v out of the plus side.
-template <int DIM, typename CT>
-__device__ __forceinline__ void flux_jumps(const CT *qm, const CT *qp, CT nx,
-                                           CT ny, CT nz, CT Zpm, CT Zsm, CT Zpp,
-                                           CT Zsp, int flux, CT *J)
+// Jump terms J = (T* - T-, v* - v-) at one face point.  qm/qp hold the
+// point's fields (velocity then stress, bfam field order); n = e_axis * sg is
+// the minus side's outward unit normal.  Upwind: exact Riemann solution of
+// the normal (P, impedance Zp) and tangential (S, impedance Zs) problems;
+// T - Z v travels out of the minus side, T + Z v out of the plus side:
+//   v*_n - v-_n = (Zp+ [v_n] + [T_n]) / (Zp- + Zp+),  T*_n - T-_n = Zp- (..)
+//   v*_t - v-_t = (Zs+ [v_t] + [T_t]) / (Zs- + Zs+),  T*_t - T-_t = Zs- (..)
+// fc = {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}, computed once per face.
+template <int DIM>
+__device__ __forceinline__ void flux_jumps(const double *qm, const double *qp,
+                                           int ax, double sg, double Zpm,
+                                           double Zsm, const double *fc,
+                                           int flux, double *J)
 {
-  CT vm[3], vp[3], Tm[3], Tp[3];
+  double vm[3], vp[3], Tm[3], Tp[3];
+  // traction S n with n = sg e_ax: column ax of S times sg (selects, so the
+  // field arrays stay in registers)
+  const bool x = ax == 0, y = ax == 1;
   if (DIM == 3)
   {
     vm[0] = qm[0]; vm[1] = qm[1]; vm[2] = qm[2];
     vp[0] = qp[0]; vp[1] = qp[1]; vp[2] = qp[2];
-    Tm[0] = qm[3] * nx + qm[6] * ny + qm[7] * nz;
-    Tm[1] = qm[6] * nx + qm[4] * ny + qm[8] * nz;
-    Tm[2] = qm[7] * nx + qm[8] * ny + qm[5] * nz;
-    Tp[0] = qp[3] * nx + qp[6] * ny + qp[7] * nz;
-    Tp[1] = qp[6] * nx + qp[4] * ny + qp[8] * nz;
-    Tp[2] = qp[7] * nx + qp[8] * ny + qp[5] * nz;
+    Tm[0] = sg * (x ? qm[3] : (y ? qm[6] : qm[7]));
+    Tm[1] = sg * (x ? qm[6] : (y ? qm[4] : qm[8]));
+    Tm[2] = sg * (x ? qm[7] : (y ? qm[8] : qm[5]));
+    Tp[0] = sg * (x ? qp[3] : (y ? qp[6] : qp[7]));
+    Tp[1] = sg * (x ? qp[6] : (y ? qp[4] : qp[8]));
+    Tp[2] = sg * (x ? qp[7] : (y ? qp[8] : qp[5]));
   }
   else
   {
     vm[0] = qm[0]; vm[1] = qm[1]; vm[2] = 0;
     vp[0] = qp[0]; vp[1] = qp[1]; vp[2] = 0;
-    Tm[0] = qm[2] * nx + qm[4] * ny;
-    Tm[1] = qm[4] * nx + qm[3] * ny;
+    Tm[0] = sg * (x ? qm[2] : qm[4]);
+    Tm[1] = sg * (x ? qm[4] : qm[3]);
     Tm[2] = 0;
-    Tp[0] = qp[2] * nx + qp[4] * ny;
-    Tp[1] = qp[4] * nx + qp[3] * ny;
+    Tp[0] = sg * (x ? qp[2] : qp[4]);
+    Tp[1] = sg * (x ? qp[4] : qp[3]);
     Tp[2] = 0;
   }
-  const CT n[3] = {nx, ny, nz};
   if (flux == 1)
   {
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-      J[a] = CT(0.5) * (Tp[a] - Tm[a]);
-      J[3 + a] = CT(0.5) * (vp[a] - vm[a]);
+      J[a] = 0.5 * (Tp[a] - Tm[a]);
+      J[3 + a] = 0.5 * (vp[a] - vm[a]);
     }
     return;
   }
-  const CT vnm = vm[0] * nx + vm[1] * ny + vm[2] * nz;
-  const CT vnp = vp[0] * nx + vp[1] * ny + vp[2] * nz;
-  const CT Tnm = Tm[0] * nx + Tm[1] * ny + Tm[2] * nz;
-  const CT Tnp = Tp[0] * nx + Tp[1] * ny + Tp[2] * nz;
-  const CT dvn = (Zpp * (vnp - vnm) + (Tnp - Tnm)) / (Zpm + Zpp);
-  const CT dTn = Zpm * dvn;
-  const CT isz = CT(1) / (Zsm + Zsp);
+  double dv[3], dT[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
   {
-    const CT dvt =
-        (Zsp * ((vp[a] - vnp * n[a]) - (vm[a] - vnm * n[a])) +
-         ((Tp[a] - Tnp * n[a]) - (Tm[a] - Tnm * n[a]))) *
-        isz;
-    J[a] = dTn * n[a] + Zsm * dvt;
-    J[3 + a] = dvn * n[a] + dvt;
+    dv[a] = vp[a] - vm[a];
+    dT[a] = Tp[a] - Tm[a];
+  }
+  // normal parts
+  const double dvn = sg * (x ? dv[0] : (y ? dv[1] : dv[2]));
+  const double dTn = sg * (x ? dT[0] : (y ? dT[1] : dT[2]));
+  const double un = (fc[0] * dvn + dTn) * fc[1];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+  {
+    const double na = a == ax ? sg : 0.0;
+    const double ut = (fc[2] * (dv[a] - dvn * na) + (dT[a] - dTn * na)) * fc[3];
+    J[a] = Zpm * un * na + Zsm * ut;
+    J[3 + a] = un * na + ut;
   }
 }
 
-// --------------------------------------------------- mortar tensor passes
+__device__ __forceinline__ void face_constants(const ElemData &me,
+                                               const ElemData &ne, double *fc)
+{
+  fc[0] = ne.Zp;
+  fc[1] = 1.0 / (me.Zp + ne.Zp);
+  fc[2] = ne.Zs;
+  fc[3] = 1.0 / (me.Zs + ne.Zs);
+}
 
-// dst[c][m + Nq*b] = sum_i A(m,i) src[c][i + Nq*b]  (face axis 0), or for
-// axis 1: dst[c][a + Nq*m] = sum_i A(m,i) src[c][a + Nq*i].  1-D faces (2D
-// volumes) only have axis 0.  A is column-major A(m,i) = A[m + Nq*i].
-template <int DIM, int N, int NT>
-__device__ __forceinline__ void face_pass(const double *A, const double *src,
-                                          double *dst, int nc, int axis,
-                                          bool accumulate)
+// slot in the 6-component jump vector of stored component c
+template <int DIM> __device__ __forceinline__ constexpr int jslot(int c)
+{
+  return c < DIM ? c : 3 + (c - DIM);
+}
+
+// In-place 1-D operator pass on a face array x[m0 + Nq*m1]:
+// axis 0: x[:, m1] <- A x[:, m1];  axis 1: x[m0, :] <- A x[m0, :].
+// A is column-major A(m,i) = A[m + Nq*i].  One thread owns one line.
+template <int N>
+__device__ __forceinline__ void line_apply(const double *A, double *x,
+                                           int stride)
 {
   constexpr int Nq = N + 1;
-  constexpr int Nfp = DIM == 3 ? Nq * Nq : Nq;
-  for (int w = threadIdx.x; w < nc * Nfp; w += NT)
+  double v[Nq], o[Nq];
+#pragma unroll
+  for (int i = 0; i < Nq; ++i)
+    v[i] = x[i * stride];
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
   {
-    const int c = w / Nfp, p = w % Nfp;
-    const int a = p % Nq, b = p / Nq;
-    const double *s = src + c * Nfp;
-    double acc = 0;
-    if (axis == 0)
-    {
+    double s = 0;
 #pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        acc += A[a + Nq * i] * s[i + Nq * b];
-    }
-    else
-    {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        acc += A[b + Nq * i] * s[a + Nq * i];
-    }
-    if (accumulate)
-      dst[w] += acc;
-    else
-      dst[w] = acc;
+    for (int i = 0; i < Nq; ++i)
+      s += A[m + Nq * i] * v[i];
+    o[m] = s;
   }
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+    x[m * stride] = o[m];
 }
 
 // ------------------------------------------------------------ the kernel
 
 template <int DIM, int N, int MODE>
-__global__ void __launch_bounds__(Shape<DIM, N>::NT)
+__global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     dg_stage_kernel(DomainView d, StageParams sp)
 {
   using S = Shape<DIM, N>;
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
-                NFLD = S::NFLD, NJ = S::NJ, NT = S::NT;
+                NFLD = S::NFLD, NJ = S::NJ, NT = S::NT, NPC = S::NPC,
+                ROWS = S::ROWS;
   extern __shared__ __align__(16) double smem[];
   double *sops = smem;
-  double *qs = smem + S::OPS_PAD;
-  double *jf = qs + S::SM_QS;
-  double *mb0 = jf + S::SM_JF;
-  double *mb1 = mb0 + S::SM_MB;
-  double *mb2 = mb1 + S::SM_MB;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(mb2 + S::SM_MB);
+  double *qs = sops + S::OPS_PAD;
+  double *dqs = qs + S::SM_QS;
+  double *pt = dqs + S::SM_DQ; // [NF][NFLD][Nfp] plus traces, then jumps
+  double *oi = pt + S::SM_PT;  // [NPC][NFLD][Nfp] own trace on mortar pieces
+  double *ms = oi + S::SM_OI;  // [NPC][NFLD][Nfp] fine partners' traces
+  double *fcf = ms + S::SM_OI; // [NF][4] face flux constants
+  double *fcp = fcf + 4 * NF;  // [NPC][4] mortar piece flux constants
+  uint64_t *bar = reinterpret_cast<uint64_t *>(fcp + 4 * NPC);
   const double *sD = sops;
   const double *sI = sops + Nq * Nq;     // interp[0..2]
   const double *sP = sops + 4 * Nq * Nq; // proj[0..2]
@@ -349,48 +397,296 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT)
   const int t = threadIdx.x;
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
+  const bool load_dq = MODE == MODE_STAGE && !sp.first_stage;
+  const ElemData me = d.ed[e];
 
-  // ---- stage the element's state into shared memory
+  // face kinds: 0 conforming, 1 glue (same size or fine side), 2 coarse side
+  int kinds = 0; // 2 bits per face
+  int coarse_mask = 0, fine_mask = 0;
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+  {
+    const int32_t nb = d.nbr[(size_t)e * NF + f];
+    int k = 0;
+    if (nb < 0)
+      k = d.gHm[-1 - nb] == 0 ? 1 : 2;
+    kinds |= k << (2 * f);
+    coarse_mask |= (k == 2) << f;
+    fine_mask |= (k == 1) << f;
+  }
+
+  // ---------------------------------------------------------- phase 0: issue
   if constexpr (S::TMA)
   {
     if (t == 0)
-      mbar_init(bar, 1);
+    {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+    }
     __syncthreads();
     if (t == 0)
     {
-      mbar_expect_tx(bar, NFLD * Np * sizeof(double));
+      mbar_expect_tx(&bar[0], NFLD * Np * sizeof(double));
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
-        bulk_g2s(qs + c * Np, d.qin + c * fs + eoff, Np * sizeof(double), bar);
+        bulk_g2s(qs + c * Np, d.qin + c * fs + eoff, Np * sizeof(double),
+                 &bar[0]);
+      if (S::DQ_SMEM && load_dq)
+      {
+        mbar_expect_tx(&bar[1], NFLD * Np * sizeof(double));
+#pragma unroll
+        for (int c = 0; c < NFLD; ++c)
+          bulk_g2s(dqs + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
+                   &bar[1]);
+      }
     }
   }
   else
   {
     for (int w = t; w < NFLD * Np; w += NT)
-      qs[w] = d.qin[(w / Np) * fs + eoff + (w % Np)];
+    {
+      cp_async8(qs + w, d.qin + (w / Np) * fs + eoff + (w % Np));
+      if (S::DQ_SMEM && load_dq)
+        cp_async8(dqs + w, d.dq + (w / Np) * fs + eoff + (w % Np));
+    }
   }
   for (int w = t; w < S::OPS; w += NT)
     sops[w] = d.ops[w];
-  double dqr[NFLD];
-  if (MODE == MODE_STAGE && t < Np)
+
+  // neighbour traces of conforming faces and coarse partners of fine-side
+  // glue faces, gathered into pt in this element's face-node order
+  for (int w = t; w < NF * Nfp; w += NT)
   {
+    const int f = w / Nfp, pn = w % Nfp;
+    const int k = (kinds >> (2 * f)) & 3;
+    if (k == 2)
+      continue;
+    const int32_t nb = d.nbr[(size_t)e * NF + f];
+    int32_t src_e;
+    int src_n;
+    if (k == 0)
+    {
+      const int code = d.nbrf[(size_t)e * NF + f];
+      src_e = nb;
+      src_n = gmask<DIM, N>(code % NF, face_perm<DIM, N>(code / NF, pn));
+    }
+    else
+    {
+      const int32_t pg = d.gEp[-1 - nb];
+      src_e = d.gEm[pg];
+      src_n = gmask<DIM, N>(d.gFm[pg], pn);
+    }
+    const double *src = d.qin + (size_t)src_e * Np + src_n;
+    double *dst = pt + f * NFLD * Nfp + pn;
 #pragma unroll
     for (int c = 0; c < NFLD; ++c)
-      dqr[c] = sp.first_stage ? 0.0 : d.dq[c * fs + eoff + t];
+      cp_async8(dst + c * Nfp, src + c * fs);
+    if (pn == 0)
+      face_constants(me, d.ed[src_e], fcf + 4 * f);
   }
-  const ElemData me = d.ed[e];
+  cp_async_commit(); // group: q (non-TMA path), dq, face traces
+
+  // fine partners of the first coarse-side face
+  auto issue_coarse = [&](int f) {
+    const int32_t g0 = -1 - d.nbr[(size_t)e * NF + f];
+    for (int w = t; w < NPC * Nfp; w += NT)
+    {
+      const int p = w / Nfp, pn = w % Nfp;
+      const int32_t pg = d.gEp[g0 + p];
+      const int32_t ep = d.gEm[pg];
+      const double *src = d.qin + (size_t)ep * Np + gmask<DIM, N>(d.gFm[pg], pn);
+      double *dst = ms + p * NFLD * Nfp + pn;
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        cp_async8(dst + c * Nfp, src + c * fs);
+      if (pn == 0)
+        face_constants(me, d.ed[ep], fcp + 4 * p);
+    }
+    cp_async_commit();
+  };
+  int next_coarse = coarse_mask ? __ffs(coarse_mask) - 1 : -1;
+  if (next_coarse >= 0)
+    issue_coarse(next_coarse);
+  else
+    cp_async_commit(); // keep the group count uniform
+
+  // ------------------------------------------------- phase 1: faces, mortars
   if constexpr (S::TMA)
   {
-    if (!mbar_wait(bar, 0))
+    if (!mbar_wait(&bar[0], 0))
       atomicExch(d.err, 1);
+  }
+  cp_async_wait<1>();
+  __syncthreads();
+
+  // fine side: coarse partner trace -> my piece, in place (rows, then columns)
+  if (fine_mask)
+  {
+    for (int pass = 0; pass < (DIM == 3 ? 2 : 1); ++pass)
+    {
+      for (int w = t; w < NF * NFLD * ROWS; w += NT)
+      {
+        const int f = w / (NFLD * ROWS), r = w % (NFLD * ROWS);
+        if (!((fine_mask >> f) & 1))
+          continue;
+        const int hp = d.gHm[d.gEp[-1 - d.nbr[(size_t)e * NF + f]]];
+        if (hp == 0)
+          continue; // same-size glue face: no interpolation
+        const int c = r / ROWS, line = r % ROWS;
+        const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
+        double *x = pt + (f * NFLD + c) * Nfp;
+        if (pass == 0)
+          line_apply<N>(sI + (1 + half) * Nq * Nq, x + Nq * line, 1);
+        else
+          line_apply<N>(sI + (1 + half) * Nq * Nq, x + line, Nq);
+      }
+      __syncthreads();
+    }
+  }
+
+  // flux on conforming and fine-side faces: read, barrier, write in place
+  {
+    double J[6];
+    int my_f = -1, my_pn = 0;
+    if (t < NF * Nfp)
+    {
+      const int f = t / Nfp, pn = t % Nfp;
+      const int k = (kinds >> (2 * f)) & 3;
+      if (k != 2)
+      {
+        my_f = f;
+        my_pn = pn;
+        const int vm = gmask<DIM, N>(f, pn);
+        int pp = pn;
+        if (k == 1)
+          pp = map_op<DIM, N>(d.gOp[-1 - d.nbr[(size_t)e * NF + f]], pn);
+        double qm[NFLD], qp[NFLD];
+        const double *x = pt + f * NFLD * Nfp;
+#pragma unroll
+        for (int c = 0; c < NFLD; ++c)
+        {
+          qm[c] = qs[c * Np + vm];
+          qp[c] = x[c * Nfp + pp];
+        }
+        flux_jumps<DIM>(qm, qp, f >> 1, (f & 1) ? 1.0 : -1.0, me.Zp, me.Zs,
+                        fcf + 4 * f, sp.flux, J);
+      }
+    }
+    __syncthreads();
+    if (my_f >= 0)
+    {
+#pragma unroll
+      for (int c = 0; c < NJ; ++c)
+        pt[(my_f * NFLD + c) * Nfp + my_pn] = J[jslot<DIM>(c)];
+    }
+  }
+
+  // coarse side: all pieces of one face at a time
+  while (next_coarse >= 0)
+  {
+    const int f = next_coarse;
+    coarse_mask &= ~(1 << f);
+    next_coarse = coarse_mask ? __ffs(coarse_mask) - 1 : -1;
+    const int32_t g0 = -1 - d.nbr[(size_t)e * NF + f];
+    cp_async_wait<0>();
+    __syncthreads(); // ms holds this face's partners; oi is free
+    // own face trace -> pieces, along face axis 0
+    for (int w = t; w < NPC * NFLD * ROWS; w += NT)
+    {
+      const int p = w / (NFLD * ROWS), r = w % (NFLD * ROWS);
+      const int c = r / ROWS, line = r % ROWS;
+      const int h = d.gHm[g0 + p];
+      const double *A = sI + (1 + ((h - 1) & 1)) * Nq * Nq;
+      double v[Nq];
+#pragma unroll
+      for (int i = 0; i < Nq; ++i)
+        v[i] = qs[c * Np + gmask<DIM, N>(f, i + Nq * line)];
+      double *x = oi + (p * NFLD + c) * Nfp + Nq * line;
+#pragma unroll
+      for (int m = 0; m < Nq; ++m)
+      {
+        double s = 0;
+#pragma unroll
+        for (int i = 0; i < Nq; ++i)
+          s += A[m + Nq * i] * v[i];
+        x[m] = s;
+      }
+    }
+    __syncthreads();
+    if (DIM == 3)
+    {
+      for (int w = t; w < NPC * NFLD * Nq; w += NT)
+      {
+        const int p = w / (NFLD * Nq), r = w % (NFLD * Nq);
+        const int c = r / Nq, col = r % Nq;
+        const int h = d.gHm[g0 + p];
+        line_apply<N>(sI + (1 + ((h - 1) >> 1)) * Nq * Nq,
+                      oi + (p * NFLD + c) * Nfp + col, Nq);
+      }
+      __syncthreads();
+    }
+    // flux on the pieces; jumps overwrite the own trace in place
+    for (int w = t; w < NPC * Nfp; w += NT)
+    {
+      const int p = w / Nfp, pn = w % Nfp;
+      const int pp = map_op<DIM, N>(d.gOp[g0 + p], pn);
+      double qm[NFLD], qp[NFLD], J[6];
+      double *x = oi + p * NFLD * Nfp;
+      const double *y = ms + p * NFLD * Nfp;
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+      {
+        qm[c] = x[c * Nfp + pn];
+        qp[c] = y[c * Nfp + pp];
+      }
+      flux_jumps<DIM>(qm, qp, f >> 1, (f & 1) ? 1.0 : -1.0, me.Zp, me.Zs,
+                      fcp + 4 * p, sp.flux, J);
+#pragma unroll
+      for (int c = 0; c < NJ; ++c)
+        x[c * Nfp + pn] = J[jslot<DIM>(c)];
+    }
+    __syncthreads(); // ms and fcp free: fetch the next face's partners
+    if (next_coarse >= 0)
+      issue_coarse(next_coarse);
+    // L2 projection back to the coarse face: axis 0, (axis 1), sum of pieces
+    for (int w = t; w < NPC * NJ * ROWS; w += NT)
+    {
+      const int p = w / (NJ * ROWS), r = w % (NJ * ROWS);
+      const int c = r / ROWS, line = r % ROWS;
+      const int h = d.gHm[g0 + p];
+      line_apply<N>(sP + (1 + ((h - 1) & 1)) * Nq * Nq,
+                    oi + (p * NFLD + c) * Nfp + Nq * line, 1);
+    }
+    __syncthreads();
+    if (DIM == 3)
+    {
+      for (int w = t; w < NPC * NJ * Nq; w += NT)
+      {
+        const int p = w / (NJ * Nq), r = w % (NJ * Nq);
+        const int c = r / Nq, col = r % Nq;
+        const int h = d.gHm[g0 + p];
+        line_apply<N>(sP + (1 + ((h - 1) >> 1)) * Nq * Nq,
+                      oi + (p * NFLD + c) * Nfp + col, Nq);
+      }
+      __syncthreads();
+    }
+    for (int w = t; w < NJ * Nfp; w += NT)
+    {
+      const int c = w / Nfp, pn = w % Nfp;
+      double s = 0;
+#pragma unroll
+      for (int p = 0; p < NPC; ++p)
+        s += oi[(p * NFLD + c) * Nfp + pn];
+      pt[(f * NFLD + c) * Nfp + pn] = s;
+    }
   }
   __syncthreads();
 
-  // ---- volume: gradients from shared memory
-  double rv[NFLD];
+  // --------------------------------------------- phase 2: volume and update
   if (t < Np)
   {
     const int i = t % Nq, j = (t / Nq) % Nq, k = t / (Nq * Nq);
+    double rv[NFLD];
     if constexpr (DIM == 3)
     {
       double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}; // d(v_c)/d(x_a): g[3c + a]
@@ -467,171 +763,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT)
       rv[3] = me.lam * div + 2 * me.mu * g[3];
       rv[4] = me.mu * (g[1] + g[2]);
     }
-  }
 
-  // ---- conforming faces: one work item per face node
-  for (int w = t; w < NF * Nfp; w += NT)
-  {
-    const int f = w / Nfp, pn = w % Nfp;
-    const int32_t nb = d.nbr[(size_t)e * NF + f];
-    if (nb < 0)
-      continue;
-    const int code = d.nbrf[(size_t)e * NF + f];
-    const int fn = code % NF, ns = code / NF;
-    const int vm = gmask<DIM, N>(f, pn);
-    const int vp = gmask<DIM, N>(fn, face_perm<DIM, N>(ns, pn));
-    const size_t noff = (size_t)nb * Np + vp;
-    double qm[NFLD], qp[NFLD];
-#pragma unroll
-    for (int c = 0; c < NFLD; ++c)
-    {
-      qm[c] = qs[c * Np + vm];
-      qp[c] = d.qin[c * fs + noff];
-    }
-    const ElemData ne = d.ed[nb];
-    const int ax = f >> 1;
-    const double sg = (f & 1) ? 1.0 : -1.0;
-    double J[NJ];
-    flux_jumps<DIM, double>(qm, qp, ax == 0 ? sg : 0.0, ax == 1 ? sg : 0.0,
-                            ax == 2 ? sg : 0.0, me.Zp, me.Zs, ne.Zp, ne.Zs,
-                            sp.flux, J);
-#pragma unroll
-    for (int c = 0; c < NJ; ++c)
-      jf[(f * NJ + c) * Nfp + pn] = J[c];
-  }
-
-  // ---- faces through the glue grid (mortars)
-  for (int f = 0; f < NF; ++f)
-  {
-    const int32_t nb = d.nbr[(size_t)e * NF + f];
-    if (nb >= 0)
-      continue; // uniform across the CTA
-    const int32_t g0 = -1 - nb;
-    const int hm0 = d.gHm[g0];
-    const int ax = f >> 1;
-    const double sg = (f & 1) ? 1.0 : -1.0;
-    const double nx = ax == 0 ? sg : 0.0, ny = ax == 1 ? sg : 0.0,
-                 nz = ax == 2 ? sg : 0.0;
-    double *jff = jf + f * NJ * Nfp;
-    if (hm0 == 0)
-    {
-      // same-size or fine side: one glue element covering the whole face
-      const int32_t pg = d.gEp[g0];
-      const int32_t ep = d.gEm[pg];
-      const int fp = d.gFm[pg], hp = d.gHm[pg], o = d.gOp[g0];
-      __syncthreads();
-      for (int w = t; w < NFLD * Nfp; w += NT)
-      {
-        const int c = w / Nfp, pn = w % Nfp;
-        mb0[w] = d.qin[c * fs + (size_t)ep * Np + gmask<DIM, N>(fp, pn)];
-      }
-      __syncthreads();
-      const double *src = mb0;
-      if (hp > 0)
-      {
-        const int a = (hp - 1) & 1, b = (hp - 1) >> 1;
-        face_pass<DIM, N, NT>(sI + (1 + a) * Nq * Nq, mb0,
-                              DIM == 3 ? mb2 : mb1, NFLD, 0, false);
-        if (DIM == 3)
-        {
-          __syncthreads();
-          face_pass<DIM, N, NT>(sI + (1 + b) * Nq * Nq, mb2, mb1, NFLD, 1,
-                                false);
-        }
-        __syncthreads();
-        src = mb1;
-      }
-      const ElemData ne = d.ed[ep];
-      for (int pn = t; pn < Nfp; pn += NT)
-      {
-        const int vm = gmask<DIM, N>(f, pn);
-        const int pp = map_op<DIM, N>(o, pn);
-        double qm[NFLD], qp[NFLD], J[NJ];
-#pragma unroll
-        for (int c = 0; c < NFLD; ++c)
-        {
-          qm[c] = qs[c * Np + vm];
-          qp[c] = src[c * Nfp + pp];
-        }
-        flux_jumps<DIM, double>(qm, qp, nx, ny, nz, me.Zp, me.Zs, ne.Zp, ne.Zs,
-                                sp.flux, J);
-#pragma unroll
-        for (int c = 0; c < NJ; ++c)
-          jff[c * Nfp + pn] = J[c];
-      }
-    }
-    else
-    {
-      // coarse side: S::NP half-size pieces, projected back and summed
-      __syncthreads();
-      for (int w = t; w < NJ * Nfp; w += NT)
-        jff[w] = 0;
-      for (int piece = 0; piece < S::NP; ++piece)
-      {
-        const int32_t g = g0 + piece;
-        const int h = d.gHm[g];
-        const int a = (h - 1) & 1, b = (h - 1) >> 1;
-        const int32_t pg = d.gEp[g];
-        const int32_t ep = d.gEm[pg];
-        const int fp = d.gFm[pg], o = d.gOp[g];
-        __syncthreads();
-        for (int w = t; w < NFLD * Nfp; w += NT)
-        {
-          const int c = w / Nfp, pn = w % Nfp;
-          mb0[w] = d.qin[c * fs + (size_t)ep * Np + gmask<DIM, N>(fp, pn)];
-          mb1[w] = qs[c * Np + gmask<DIM, N>(f, pn)];
-        }
-        __syncthreads();
-        face_pass<DIM, N, NT>(sI + (1 + a) * Nq * Nq, mb1, mb2, NFLD, 0,
-                              false);
-        __syncthreads();
-        const double *qmi = mb2;
-        if (DIM == 3)
-        {
-          face_pass<DIM, N, NT>(sI + (1 + b) * Nq * Nq, mb2, mb1, NFLD, 1,
-                                false);
-          __syncthreads();
-          qmi = mb1;
-        }
-        const ElemData ne = d.ed[ep];
-        // jump terms go to the buffer that holds neither trace
-        double *Jm = DIM == 3 ? mb2 : mb1;
-        for (int pn = t; pn < Nfp; pn += NT)
-        {
-          const int pp = map_op<DIM, N>(o, pn);
-          double qm[NFLD], qp[NFLD], J[NJ];
-#pragma unroll
-          for (int c = 0; c < NFLD; ++c)
-          {
-            qm[c] = qmi[c * Nfp + pn];
-            qp[c] = mb0[c * Nfp + pp];
-          }
-          flux_jumps<DIM, double>(qm, qp, nx, ny, nz, me.Zp, me.Zs, ne.Zp,
-                                  ne.Zs, sp.flux, J);
-#pragma unroll
-          for (int c = 0; c < NJ; ++c)
-            Jm[c * Nfp + pn] = J[c];
-        }
-        __syncthreads();
-        if (DIM == 3)
-        {
-          face_pass<DIM, N, NT>(sP + (1 + a) * Nq * Nq, Jm, mb0, NJ, 0, false);
-          __syncthreads();
-          face_pass<DIM, N, NT>(sP + (1 + b) * Nq * Nq, mb0, jff, NJ, 1, true);
-        }
-        else
-        {
-          face_pass<DIM, N, NT>(sP + (1 + a) * Nq * Nq, Jm, jff, NJ, 0, true);
-        }
-      }
-    }
-  }
-  __syncthreads();
-
-  // ---- lift (lumped LGL mass), combine, stage update
-  if (t < Np)
-  {
-    const int i = t % Nq, j = (t / Nq) % Nq, k = t / (Nq * Nq);
+    // lift of the face jump terms with the lumped LGL mass
     const double iwend = 1.0 / sw[0];
     const double r3[3] = {me.rx, me.ry, me.rz};
 #pragma unroll
@@ -646,9 +779,11 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT)
                               : (ax == 0 ? j : i);
       const double L = r3[ax] * iwend;
       const double sg = side ? 1.0 : -1.0;
-      const double *Jf = jf + f * NJ * Nfp + pn;
-      const double dT0 = Jf[0 * Nfp], dT1 = Jf[1 * Nfp], dT2 = Jf[2 * Nfp];
-      const double dv0 = Jf[3 * Nfp], dv1 = Jf[4 * Nfp], dv2 = Jf[5 * Nfp];
+      const double *Jf = pt + f * NFLD * Nfp + pn;
+      const double dT0 = Jf[0 * Nfp], dT1 = Jf[1 * Nfp];
+      const double dT2 = DIM == 3 ? Jf[2 * Nfp] : 0.0;
+      const double dv0 = Jf[DIM * Nfp], dv1 = Jf[(DIM + 1) * Nfp];
+      const double dv2 = DIM == 3 ? Jf[5 * Nfp] : 0.0;
       const double dvv[3] = {dv0, dv1, dv2};
       const double dvn = sg * dvv[ax];
       if constexpr (DIM == 3)
@@ -674,12 +809,40 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT)
         rv[4] += lm * (ax == 1 ? dv0 : 0.0) + lm * (ax == 0 ? dv1 : 0.0);
       }
     }
+
     if constexpr (MODE == MODE_STAGE)
     {
+      double dqo[NFLD];
+      if (load_dq)
+      {
+        if constexpr (S::DQ_SMEM)
+        {
+          if constexpr (S::TMA)
+          {
+            if (!mbar_wait(&bar[1], 0))
+              atomicExch(d.err, 2);
+          }
+#pragma unroll
+          for (int c = 0; c < NFLD; ++c)
+            dqo[c] = dqs[c * Np + t];
+        }
+        else
+        {
+#pragma unroll
+          for (int c = 0; c < NFLD; ++c)
+            dqo[c] = d.dq[c * fs + eoff + t];
+        }
+      }
+      else
+      {
+#pragma unroll
+        for (int c = 0; c < NFLD; ++c)
+          dqo[c] = 0.0;
+      }
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
       {
-        const double dqn = sp.A * dqr[c] + sp.dt * rv[c];
+        const double dqn = sp.A * dqo[c] + sp.dt * rv[c];
         d.dq[c * fs + eoff + t] = dqn;
         d.qout[c * fs + eoff + t] = qs[c * Np + t] + sp.B * dqn;
       }
