@@ -5,7 +5,8 @@
 // material and operators, owns the device state and launches the fused
 // stage kernel once per LSRK stage (optionally replayed from a CUDA graph).
 #include "bfam_gpu.h"
-#include "dg_kernels.cuh"
+#include "dg_energy.cuh"
+#include "dg_stage.cuh"
 
 #include <atomic>
 #include <cmath>
@@ -43,25 +44,57 @@ int fail(int code, const char *fmt, ...)
                   cudaGetErrorString(e_), __FILE__, __LINE__);                 \
   } while (0)
 
-typedef void (*stage_fn)(DomainView, StageParams);
+// per-order launchers (the kernels' parameter lists depend on the order)
+typedef void (*stage_launch_fn)(const DomainView &, const StageParams &,
+                                const double *D, int mode, cudaStream_t);
+typedef cudaError_t (*prepare_fn)();
 typedef void (*energy_fn)(const double *, size_t, const ElemData *,
                           const double *, double *);
 
 struct KernelSet
 {
-  stage_fn stage = nullptr;
-  stage_fn rhs = nullptr;
+  stage_launch_fn launch = nullptr;
+  prepare_fn prepare = nullptr;
   energy_fn energy = nullptr;
   int NT = 0;
   size_t smem = 0;
 };
 
+template <int DIM, int N>
+void stage_launch(const DomainView &v, const StageParams &sp, const double *D,
+                  int mode, cudaStream_t stream)
+{
+  using S = Shape<DIM, N>;
+  DiffOp<N> dop;
+  for (int i = 0; i < (N + 1) * (N + 1); ++i)
+    dop.D[i] = D[i];
+  const size_t smem = (size_t)S::SM_TOTAL * sizeof(double);
+  if (mode == MODE_STAGE)
+    dg_stage_kernel<DIM, N, MODE_STAGE><<<v.K, S::NT, smem, stream>>>(v, sp, dop);
+  else
+    dg_stage_kernel<DIM, N, MODE_RHS><<<v.K, S::NT, smem, stream>>>(v, sp, dop);
+}
+
+template <int DIM, int N> cudaError_t stage_prepare()
+{
+  using S = Shape<DIM, N>;
+  const int smem = (int)(S::SM_TOTAL * sizeof(double));
+  cudaError_t e = cudaFuncSetAttribute(
+      (const void *)dg_stage_kernel<DIM, N, MODE_STAGE>,
+      cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute((const void *)dg_stage_kernel<DIM, N, MODE_RHS>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              smem);
+}
+
 template <int DIM, int N> KernelSet make_set()
 {
   using S = Shape<DIM, N>;
   KernelSet k;
-  k.stage = dg_stage_kernel<DIM, N, MODE_STAGE>;
-  k.rhs = dg_stage_kernel<DIM, N, MODE_RHS>;
+  k.launch = stage_launch<DIM, N>;
+  k.prepare = stage_prepare<DIM, N>;
   k.energy = dg_energy_kernel<DIM, N>;
   k.NT = S::NT;
   k.smem = (size_t)S::SM_TOTAL * sizeof(double);
@@ -145,11 +178,10 @@ struct bfam_gpu_domain
   double *rhs = nullptr;
   double *energy = nullptr;
   ElemData *ed = nullptr;
-  int32_t *nbr = nullptr;
-  int8_t *nbrf = nullptr;
-  int32_t *gEm = nullptr, *gEp = nullptr;
-  int8_t *gFm = nullptr, *gHm = nullptr, *gOp = nullptr;
+  int2 *fdesc = nullptr;
+  int2 *gpart = nullptr;
   double *ops = nullptr;
+  std::vector<double> Dr; // host copy, passed by value to each launch
   int *err = nullptr;
   int cur = 0;
   size_t bytes = 0, budget = 0;
@@ -222,13 +254,8 @@ DomainView view(bfam_gpu_domain_t *d, int in)
   v.dq = d->dq;
   v.rhs = d->rhs;
   v.ed = d->ed;
-  v.nbr = d->nbr;
-  v.nbrf = d->nbrf;
-  v.gEm = d->gEm;
-  v.gEp = d->gEp;
-  v.gFm = d->gFm;
-  v.gHm = d->gHm;
-  v.gOp = d->gOp;
+  v.fdesc = d->fdesc;
+  v.gpart = d->gpart;
   v.ops = d->ops;
   v.err = d->err;
   return v;
@@ -244,8 +271,7 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double dt,
   sp.first_stage = first;
   sp.flux = d->flux;
   DomainView v = view(d, in);
-  stage_fn fn = mode == MODE_STAGE ? d->ks.stage : d->ks.rhs;
-  fn<<<d->K, d->ks.NT, d->ks.smem, d->stream>>>(v, sp);
+  d->ks.launch(v, sp, d->Dr.data(), mode, d->stream);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   CUDA_TRY(cudaGetLastError());
   return 0;
@@ -418,6 +444,37 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
                   "element",
                   i / NF, i % NF);
 
+  // ---- compact descriptors read by the kernel (layout in dg_common.cuh)
+  std::vector<int2> fdesc((size_t)K * NF);
+  for (size_t i = 0; i < fdesc.size(); ++i)
+  {
+    const int32_t nb = nbr[i];
+    if (nb >= 0)
+    {
+      const int code = nbrf[i];
+      fdesc[i] = make_int2(nb, 0 | ((code % NF) << 2) | ((code / NF) << 5));
+      continue;
+    }
+    const int32_t g0 = -1 - nb;
+    if (glue->EToHm[g0] == 0)
+    {
+      const int32_t pg = glue->EToEp[g0];
+      fdesc[i] = make_int2(glue->EToEm[pg], 1 | (glue->EToFm[pg] << 2) |
+                                                (glue->EToOp[g0] << 5) |
+                                                (glue->EToHm[pg] << 8));
+    }
+    else
+      fdesc[i] = make_int2(g0, 2);
+  }
+  std::vector<int2> gpart(Kg > 0 ? Kg : 1, make_int2(0, 0));
+  for (int32_t g = 0; g < Kg; ++g)
+  {
+    const int32_t pg = glue->EToEp[g];
+    gpart[g] = make_int2(glue->EToEm[pg], glue->EToFm[pg] |
+                                              (glue->EToOp[g] << 3) |
+                                              (glue->EToHm[g] << 6));
+  }
+
   // ---- operators: Dr | interp[3] | proj[3] | w
   std::vector<double> ops(7 * Nq * Nq + Nq, 0.0);
   std::memcpy(ops.data(), vol->Dr, sizeof(double) * Nq * Nq);
@@ -515,35 +572,22 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
       return fail(BFAM_GPU_ECUDA, "stream: %s", cudaGetErrorString(ce));
     }
     d->own_stream = true;
-    for (stage_fn fn : {ks.stage, ks.rhs})
+    ce = ks.prepare();
+    if (ce != cudaSuccess)
     {
-      ce = cudaFuncSetAttribute((const void *)fn,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)ks.smem);
-      if (ce != cudaSuccess)
-      {
-        release(d);
-        return fail(BFAM_GPU_ECUDA, "smem attribute: %s",
-                    cudaGetErrorString(ce));
-      }
+      release(d);
+      return fail(BFAM_GPU_ECUDA, "smem attribute: %s", cudaGetErrorString(ce));
     }
   }
+  d->Dr.assign(vol->Dr, vol->Dr + Nq * Nq);
   const size_t state = (size_t)NFLD * d->fs * sizeof(double);
   TRY(dev_alloc(d, (void **)&d->q[0], state));
   TRY(dev_alloc(d, (void **)&d->q[1], state));
   TRY(dev_alloc(d, (void **)&d->dq, state));
   TRY(upload(d, &d->ed, ed.data(), ed.size()));
-  TRY(upload(d, &d->nbr, nbr.data(), nbr.size()));
-  TRY(upload(d, &d->nbrf, nbrf.data(), nbrf.size()));
+  TRY(upload(d, &d->fdesc, fdesc.data(), fdesc.size()));
+  TRY(upload(d, &d->gpart, gpart.data(), gpart.size()));
   TRY(upload(d, &d->ops, ops.data(), ops.size()));
-  if (Kg > 0)
-  {
-    TRY(upload(d, &d->gEm, glue->EToEm, Kg));
-    TRY(upload(d, &d->gEp, glue->EToEp, Kg));
-    TRY(upload(d, &d->gFm, glue->EToFm, Kg));
-    TRY(upload(d, &d->gHm, glue->EToHm, Kg));
-    TRY(upload(d, &d->gOp, glue->EToOp, Kg));
-  }
   TRY(dev_alloc(d, (void **)&d->err, sizeof(int)));
 #undef TRY
   if (cudaMemset(d->q[0], 0, state) != cudaSuccess ||

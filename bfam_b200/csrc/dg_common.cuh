@@ -1,0 +1,367 @@
+// Shared definitions of the sm_100a kernels: device-side views of a domain,
+// per-order shapes, PTX wrappers (TMA bulk copies, cp.async, mbarrier),
+// bfam's face numbering, the elastic upwind flux and small 1-D operator
+// passes.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bfam_b200
+{
+
+struct ElemData
+{
+  double irho, lam, mu, Zp, Zs, rx, ry, rz; // rx = 2/hx, ...
+};
+
+// Face descriptor, one per (element, face), built on the host from vmapP and
+// the glue grid.  b & 3 is the kind:
+//   0 conforming:        a = neighbour element, b>>2 & 7 = its face,
+//                        b>>5 & 7 = node permutation code
+//   1 glue, whole face:  a = partner element (same size or coarse),
+//                        b>>2 & 7 = partner face, b>>5 & 7 = glue orientation,
+//                        b>>8 & 7 = partner's hanging piece (0: same size)
+//   2 glue, coarse side: a = first of the face's glue elements
+// Glue partner, one per glue element g (used on the coarse side):
+//   a = partner (fine) element, b & 7 = partner face, b>>3 & 7 = orientation,
+//   b>>6 & 7 = hanging piece of g.
+struct DomainView
+{
+  int32_t K;
+  size_t fs; // field stride K*Np
+  const double *__restrict__ qin;
+  double *__restrict__ qout;
+  double *__restrict__ dq;
+  double *__restrict__ rhs; // right-hand-side output (rhs mode)
+  const ElemData *__restrict__ ed;
+  const int2 *__restrict__ fdesc; // [K][NF]
+  const int2 *__restrict__ gpart; // [Kg]
+  const double *__restrict__ ops;  // Dr | interp[3] | proj[3] | w
+  int *err;
+};
+
+struct StageParams
+{
+  double A, B, dt;
+  int first_stage; // A == 0: dq is not read
+  int flux;        // 0 upwind, 1 central
+};
+
+// The 1-D differentiation matrix travels in the kernel's parameter space so
+// that its entries, indexed by unrolled loop counters, are constant-bank
+// operands of the FMAs.
+template <int N> struct DiffOp
+{
+  double D[(N + 1) * (N + 1)]; // column-major D(i,m) = D[i + (N+1) m]
+};
+
+enum
+{
+  MODE_STAGE = 0,
+  MODE_RHS = 1
+};
+
+template <int DIM, int N> struct Shape
+{
+  static constexpr int Nq = N + 1;
+  static constexpr int Np = DIM == 3 ? Nq * Nq * Nq : Nq * Nq;
+  static constexpr int Nfp = DIM == 3 ? Nq * Nq : Nq;
+  static constexpr int NF = 2 * DIM;
+  static constexpr int NFLD = DIM == 3 ? 9 : 5;
+  // stored jump components: (T* - T-)[0..DIM), (v* - v-)[0..DIM)
+  static constexpr int NJ = 2 * DIM;
+  static constexpr int NPC = DIM == 3 ? 4 : 2; // mortar pieces per coarse face
+  static constexpr int ROWS = DIM == 3 ? Nq : 1; // rows of a face
+  static constexpr int NL = Np / Nq;              // lines per direction
+  static constexpr int NDF = DIM == 3 ? 6 : 4; // fields differentiated per axis
+  static constexpr int work = (Np > NF * Nfp ? Np : NF * Nfp);
+  static constexpr int NT = ((work + 31) / 32) * 32 > 1024
+                                ? 1024
+                                : ((work + 31) / 32) * 32;
+  // CTAs per SM the register allocation is sized for (about 96 registers)
+  static constexpr int MINB_RAW = 65536 / (NT * 96);
+  static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW);
+  static constexpr int OPS = 7 * Nq * Nq + Nq;
+  static constexpr int OPS_PAD = (OPS + 1) & ~1; // keep 16-byte alignment
+  static constexpr bool TMA = (Np % 2) == 0;     // 16-byte aligned element rows
+  static constexpr bool DQ_SMEM = NFLD * Np * 8 <= 20 * 1024;
+  // shared memory regions in doubles (all even, so 16-byte aligned)
+  static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2;
+  static constexpr int SM_DQ = DQ_SMEM ? SM_QS : 0;
+  static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
+  static constexpr int SM_OI = NPC * NFLD * Nfp + (NPC * NFLD * Nfp) % 2;
+  // mortar scratch (own trace on pieces, partner traces); reused afterwards
+  // for the volume right-hand side
+  static constexpr int SM_MOR = 2 * SM_OI > SM_QS ? 2 * SM_OI : SM_QS;
+  static constexpr int SM_FC = 4 * (NF + NPC);
+  static constexpr int SM_TOTAL =
+      OPS_PAD + SM_QS + SM_DQ + SM_PT + SM_MOR + SM_FC + 4;
+};
+
+// ------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
+                                         uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::"
+               "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// 8-byte asynchronous gather global -> shared (completes with the group)
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)),
+               "l"(src)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit()
+{
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int NPENDING> __device__ __forceinline__ void cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;" ::"n"(NPENDING) : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait on phase `parity`; gives up after ~2 s of wall time and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+  const uint32_t a = smem_u32(bar);
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it)
+  {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(a), "r"(parity)
+                 : "memory");
+    if (done)
+      return true;
+    if (it == 0)
+      t0 = global_ns();
+    else if ((it & 63) == 0 && global_ns() - t0 > 2000000000ull)
+      return false;
+  }
+}
+
+// --------------------------------------------------------- index helpers
+
+// volume node of face node pn on face f (bfam face masks)
+template <int DIM, int N> __device__ __forceinline__ int gmask(int f, int pn)
+{
+  constexpr int Nq = N + 1;
+  if (DIM == 2)
+  {
+    switch (f)
+    {
+    case 0: return pn * Nq;
+    case 1: return pn * Nq + N;
+    case 2: return pn;
+    default: return N * Nq + pn;
+    }
+  }
+  const int a = pn % Nq, b = pn / Nq;
+  switch (f)
+  {
+  case 0: return Nq * a + Nq * Nq * b;
+  case 1: return N + Nq * a + Nq * Nq * b;
+  case 2: return a + Nq * Nq * b;
+  case 3: return a + Nq * N + Nq * Nq * b;
+  case 4: return a + Nq * b;
+  default: return a + Nq * b + Nq * Nq * N;
+  }
+}
+
+// neighbour face-node of my face node pn under permutation code ns
+// (bfam_subdomain_dgx_buildmaps, src/bfam.c:6823-6866)
+template <int DIM, int N> __device__ __forceinline__ int face_perm(int ns, int pn)
+{
+  constexpr int Nq = N + 1;
+  if (DIM == 2)
+    return ns ? N - pn : pn;
+  const int i = pn % Nq, j = pn / Nq, ir = N - i, jr = N - j;
+  switch (ns)
+  {
+  case 0: return i + j * Nq;
+  case 1: return j + i * Nq;
+  case 2: return ir + j * Nq;
+  case 3: return jr + i * Nq;
+  case 4: return j + ir * Nq;
+  case 5: return i + jr * Nq;
+  case 6: return jr + ir * Nq;
+  default: return ir + jr * Nq;
+  }
+}
+
+// glue orientation map mapOp[o][n] (src/bfam.c:7430-7461)
+template <int DIM, int N> __device__ __forceinline__ int map_op(int o, int pn)
+{
+  constexpr int Nq = N + 1;
+  if (DIM == 2)
+    return o ? N - pn : pn;
+  const int i = pn % Nq, j = pn / Nq, ir = N - i, jr = N - j;
+  switch (o)
+  {
+  case 0: return i + j * Nq;
+  case 1: return j + i * Nq;
+  case 2: return ir + j * Nq;
+  case 3: return j + ir * Nq;
+  case 4: return jr + i * Nq;
+  case 5: return i + jr * Nq;
+  case 6: return jr + ir * Nq;
+  default: return ir + jr * Nq;
+  }
+}
+
+// ------------------------------------------------------------- physics
+
+// Jump terms J = (T* - T-, v* - v-) at one face point.  qm/qp hold the
+// point's fields (velocity then stress, bfam field order); n = e_axis * sg is
+// the minus side's outward unit normal.  Upwind: exact Riemann solution of
+// the normal (P, impedance Zp) and tangential (S, impedance Zs) problems;
+// T - Z v travels out of the minus side, T + Z v out of the plus side:
+//   v*_n - v-_n = (Zp+ [v_n] + [T_n]) / (Zp- + Zp+),  T*_n - T-_n = Zp- (..)
+//   v*_t - v-_t = (Zs+ [v_t] + [T_t]) / (Zs- + Zs+),  T*_t - T-_t = Zs- (..)
+// fc = {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}, computed once per face.
+template <int DIM>
+__device__ __forceinline__ void flux_jumps(const double *qm, const double *qp,
+                                           int ax, double sg, double Zpm,
+                                           double Zsm, const double *fc,
+                                           int flux, double *J)
+{
+  double vm[3], vp[3], Tm[3], Tp[3];
+  // traction S n with n = sg e_ax: column ax of S times sg (selects, so the
+  // field arrays stay in registers)
+  const bool x = ax == 0, y = ax == 1;
+  if (DIM == 3)
+  {
+    vm[0] = qm[0]; vm[1] = qm[1]; vm[2] = qm[2];
+    vp[0] = qp[0]; vp[1] = qp[1]; vp[2] = qp[2];
+    Tm[0] = sg * (x ? qm[3] : (y ? qm[6] : qm[7]));
+    Tm[1] = sg * (x ? qm[6] : (y ? qm[4] : qm[8]));
+    Tm[2] = sg * (x ? qm[7] : (y ? qm[8] : qm[5]));
+    Tp[0] = sg * (x ? qp[3] : (y ? qp[6] : qp[7]));
+    Tp[1] = sg * (x ? qp[6] : (y ? qp[4] : qp[8]));
+    Tp[2] = sg * (x ? qp[7] : (y ? qp[8] : qp[5]));
+  }
+  else
+  {
+    vm[0] = qm[0]; vm[1] = qm[1]; vm[2] = 0;
+    vp[0] = qp[0]; vp[1] = qp[1]; vp[2] = 0;
+    Tm[0] = sg * (x ? qm[2] : qm[4]);
+    Tm[1] = sg * (x ? qm[4] : qm[3]);
+    Tm[2] = 0;
+    Tp[0] = sg * (x ? qp[2] : qp[4]);
+    Tp[1] = sg * (x ? qp[4] : qp[3]);
+    Tp[2] = 0;
+  }
+  if (flux == 1)
+  {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+      J[a] = 0.5 * (Tp[a] - Tm[a]);
+      J[3 + a] = 0.5 * (vp[a] - vm[a]);
+    }
+    return;
+  }
+  double dv[3], dT[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+  {
+    dv[a] = vp[a] - vm[a];
+    dT[a] = Tp[a] - Tm[a];
+  }
+  // normal parts
+  const double dvn = sg * (x ? dv[0] : (y ? dv[1] : dv[2]));
+  const double dTn = sg * (x ? dT[0] : (y ? dT[1] : dT[2]));
+  const double un = (fc[0] * dvn + dTn) * fc[1];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+  {
+    const double na = a == ax ? sg : 0.0;
+    const double ut = (fc[2] * (dv[a] - dvn * na) + (dT[a] - dTn * na)) * fc[3];
+    J[a] = Zpm * un * na + Zsm * ut;
+    J[3 + a] = un * na + ut;
+  }
+}
+
+__device__ __forceinline__ void face_constants(const ElemData &me,
+                                               const ElemData &ne, double *fc)
+{
+  fc[0] = ne.Zp;
+  fc[1] = 1.0 / (me.Zp + ne.Zp);
+  fc[2] = ne.Zs;
+  fc[3] = 1.0 / (me.Zs + ne.Zs);
+}
+
+// slot in the 6-component jump vector of stored component c
+template <int DIM> __device__ __forceinline__ constexpr int jslot(int c)
+{
+  return c < DIM ? c : 3 + (c - DIM);
+}
+
+// In-place 1-D operator pass on a face array x[m0 + Nq*m1]:
+// axis 0: x[:, m1] <- A x[:, m1];  axis 1: x[m0, :] <- A x[m0, :].
+// A is column-major A(m,i) = A[m + Nq*i].  One thread owns one line.
+template <int N>
+__device__ __forceinline__ void line_apply(const double *A, double *x,
+                                           int stride)
+{
+  constexpr int Nq = N + 1;
+  double v[Nq], o[Nq];
+#pragma unroll
+  for (int i = 0; i < Nq; ++i)
+    v[i] = x[i * stride];
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+  {
+    double s = 0;
+#pragma unroll
+    for (int i = 0; i < Nq; ++i)
+      s += A[m + Nq * i] * v[i];
+    o[m] = s;
+  }
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+    x[m * stride] = o[m];
+}
+
+
+} // namespace bfam_b200
