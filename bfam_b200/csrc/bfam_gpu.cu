@@ -60,14 +60,17 @@ struct KernelSet
   size_t smem = 0;
 };
 
+// hops: host copy of the operator block Dr | interp[3] | proj[3] | w
 template <int DIM, int N>
-void stage_launch(const DomainView &v, const StageParams &sp, const double *D,
-                  int mode, cudaStream_t stream)
+void stage_launch(const DomainView &v, const StageParams &sp,
+                  const double *hops, int mode, cudaStream_t stream)
 {
   using S = Shape<DIM, N>;
+  constexpr int n2 = (N + 1) * (N + 1);
   DiffOp<N> dop;
-  for (int i = 0; i < (N + 1) * (N + 1); ++i)
-    dop.D[i] = D[i];
+  for (int i = 0; i < n2; ++i)
+    dop.D[i] = hops[i];
+  dop.iwend = 1.0 / hops[7 * n2];
   const size_t smem = (size_t)S::SM_TOTAL * sizeof(double);
   if (mode == MODE_STAGE)
     dg_stage_kernel<DIM, N, MODE_STAGE><<<v.K, S::NT, smem, stream>>>(v, sp, dop);
@@ -180,8 +183,12 @@ struct bfam_gpu_domain
   ElemData *ed = nullptr;
   int2 *fdesc = nullptr;
   int2 *gpart = nullptr;
+  double4 *fcE = nullptr;
+  double4 *fcG = nullptr;
   double *ops = nullptr;
-  std::vector<double> Dr; // host copy, passed by value to each launch
+  // host copy of Dr | interp[3] | proj[3] | w; the 1-D operators are passed
+  // by value (kernel parameter bank) to each launch
+  std::vector<double> hops;
   int *err = nullptr;
   int cur = 0;
   size_t bytes = 0, budget = 0;
@@ -256,6 +263,8 @@ DomainView view(bfam_gpu_domain_t *d, int in)
   v.ed = d->ed;
   v.fdesc = d->fdesc;
   v.gpart = d->gpart;
+  v.fcE = d->fcE;
+  v.fcG = d->fcG;
   v.ops = d->ops;
   v.err = d->err;
   return v;
@@ -271,7 +280,7 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double dt,
   sp.first_stage = first;
   sp.flux = d->flux;
   DomainView v = view(d, in);
-  d->ks.launch(v, sp, d->Dr.data(), mode, d->stream);
+  d->ks.launch(v, sp, d->hops.data(), mode, d->stream);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   CUDA_TRY(cudaGetLastError());
   return 0;
@@ -526,6 +535,19 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
     }
   }
 
+  // ---- upwind flux constants of every face and glue element
+  auto fconst = [&](int32_t me, int32_t nb) {
+    return make_double4(ed[nb].Zp, 1.0 / (ed[me].Zp + ed[nb].Zp), ed[nb].Zs,
+                        1.0 / (ed[me].Zs + ed[nb].Zs));
+  };
+  std::vector<double4> fcE((size_t)K * NF, make_double4(0, 0, 0, 0));
+  for (size_t i = 0; i < fcE.size(); ++i)
+    if ((fdesc[i].y & 3) != 2)
+      fcE[i] = fconst((int32_t)(i / NF), fdesc[i].x);
+  std::vector<double4> fcG(Kg > 0 ? Kg : 1, make_double4(0, 0, 0, 0));
+  for (int32_t g = 0; g < Kg; ++g)
+    fcG[g] = fconst(glue->EToEm[g], glue->EToEm[glue->EToEp[g]]);
+
   // ---- device
   bfam_gpu_domain_t *d = new bfam_gpu_domain_t();
   d->dim = dim;
@@ -579,7 +601,7 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
       return fail(BFAM_GPU_ECUDA, "smem attribute: %s", cudaGetErrorString(ce));
     }
   }
-  d->Dr.assign(vol->Dr, vol->Dr + Nq * Nq);
+  d->hops = ops;
   const size_t state = (size_t)NFLD * d->fs * sizeof(double);
   TRY(dev_alloc(d, (void **)&d->q[0], state));
   TRY(dev_alloc(d, (void **)&d->q[1], state));
@@ -587,6 +609,8 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
   TRY(upload(d, &d->ed, ed.data(), ed.size()));
   TRY(upload(d, &d->fdesc, fdesc.data(), fdesc.size()));
   TRY(upload(d, &d->gpart, gpart.data(), gpart.size()));
+  TRY(upload(d, &d->fcE, fcE.data(), fcE.size()));
+  TRY(upload(d, &d->fcG, fcG.data(), fcG.size()));
   TRY(upload(d, &d->ops, ops.data(), ops.size()));
   TRY(dev_alloc(d, (void **)&d->err, sizeof(int)));
 #undef TRY

@@ -37,6 +37,9 @@ struct DomainView
   const ElemData *__restrict__ ed;
   const int2 *__restrict__ fdesc; // [K][NF]
   const int2 *__restrict__ gpart; // [Kg]
+  // upwind flux constants {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}:
+  const double4 *__restrict__ fcE; // [K][NF] conforming / whole-face glue
+  const double4 *__restrict__ fcG; // [Kg] per glue element (coarse side)
   const double *__restrict__ ops;  // Dr | interp[3] | proj[3] | w
   int *err;
 };
@@ -48,12 +51,13 @@ struct StageParams
   int flux;        // 0 upwind, 1 central
 };
 
-// The 1-D differentiation matrix travels in the kernel's parameter space so
-// that its entries, indexed by unrolled loop counters, are constant-bank
-// operands of the FMAs.
+// The 1-D operators travel in the kernel's parameter space so that their
+// entries, indexed by unrolled loop counters, are constant-bank operands of
+// the FMAs.  All column-major, A(i,m) = A[i + (N+1) m].
 template <int N> struct DiffOp
 {
-  double D[(N + 1) * (N + 1)]; // column-major D(i,m) = D[i + (N+1) m]
+  double D[(N + 1) * (N + 1)]; // LGL differentiation
+  double iwend;                // 1 / w_0, the lumped-mass face weight
 };
 
 enum
@@ -82,21 +86,18 @@ template <int DIM, int N> struct Shape
   // CTAs per SM the register allocation is sized for (about 96 registers)
   static constexpr int MINB_RAW = 65536 / (NT * 96);
   static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW);
-  static constexpr int OPS = 7 * Nq * Nq + Nq;
-  static constexpr int OPS_PAD = (OPS + 1) & ~1; // keep 16-byte alignment
-  static constexpr bool TMA = (Np % 2) == 0;     // 16-byte aligned element rows
-  static constexpr bool DQ_SMEM = NFLD * Np * 8 <= 20 * 1024;
+  static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
   // shared memory regions in doubles (all even, so 16-byte aligned)
-  static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2;
-  static constexpr int SM_DQ = DQ_SMEM ? SM_QS : 0;
+  static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q
+  static constexpr int SM_DQ = SM_QS; // dq, then A dq + dt rhs in place
   static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
   static constexpr int SM_OI = NPC * NFLD * Nfp + (NPC * NFLD * Nfp) % 2;
-  // mortar scratch (own trace on pieces, partner traces); reused afterwards
-  // for the volume right-hand side
-  static constexpr int SM_MOR = 2 * SM_OI > SM_QS ? 2 * SM_OI : SM_QS;
+  // mortar scratch: own trace on the pieces, fine partners' traces
+  static constexpr int SM_MOR = 2 * SM_OI;
   static constexpr int SM_FC = 4 * (NF + NPC);
+  static constexpr int SM_IP = 4 * Nq * Nq; // interp (bottom, top), proj (.., ..)
   static constexpr int SM_TOTAL =
-      OPS_PAD + SM_QS + SM_DQ + SM_PT + SM_MOR + SM_FC + 4;
+      SM_QS + SM_DQ + SM_PT + SM_MOR + SM_FC + SM_IP + 4;
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -337,9 +338,26 @@ template <int DIM> __device__ __forceinline__ constexpr int jslot(int c)
   return c < DIM ? c : 3 + (c - DIM);
 }
 
-// In-place 1-D operator pass on a face array x[m0 + Nq*m1]:
-// axis 0: x[:, m1] <- A x[:, m1];  axis 1: x[m0, :] <- A x[m0, :].
-// A is column-major A(m,i) = A[m + Nq*i].  One thread owns one line.
+// out[m] = sum_i A(m,i) v[i], A column-major in shared memory
+template <int N>
+__device__ __forceinline__ void apply_smem(const double *A, const double *v,
+                                           double *out)
+{
+  constexpr int Nq = N + 1;
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+  {
+    double s = 0;
+#pragma unroll
+    for (int i = 0; i < Nq; ++i)
+      s += A[m + Nq * i] * v[i];
+    out[m] = s;
+  }
+}
+
+// In-place 1-D operator pass on one line of a face array x[m0 + Nq*m1]
+// (stride 1: along face axis 0, stride Nq: along axis 1).  One thread owns
+// one line.
 template <int N>
 __device__ __forceinline__ void line_apply(const double *A, double *x,
                                            int stride)
@@ -349,18 +367,18 @@ __device__ __forceinline__ void line_apply(const double *A, double *x,
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
     v[i] = x[i * stride];
-#pragma unroll
-  for (int m = 0; m < Nq; ++m)
-  {
-    double s = 0;
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-      s += A[m + Nq * i] * v[i];
-    o[m] = s;
-  }
+  apply_smem<N>(A, v, o);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
     x[m * stride] = o[m];
+}
+
+// 16-byte asynchronous copy global -> shared (both 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)),
+               "l"(src)
+               : "memory");
 }
 
 

@@ -2,12 +2,17 @@
 // affine Cartesian elements (sm_100a).
 //
 // One launch per LSRK stage does, per element (one CTA per element):
-//   gather  : every global read of the element is issued up front -- its own
-//             state q (and dq) by TMA bulk copies into shared memory, the
-//             neighbours' face traces by 8-byte cp.async gathers straight into
-//             shared memory, addressed from a per-face descriptor.  This is the
+//   issue   : every global read of the element is issued up front -- its own
+//             q and dq by TMA bulk copies into shared memory, the neighbours'
+//             face traces by 8-byte cp.async gathers straight into shared
+//             memory, addressed from a per-face descriptor.  This is the
 //             on-device replacement of vmapP and of the bfam_communicator
 //             ghost exchange (src/bfam.c:6783-6877, 2418-2679);
+//   volume  : while the gathers are in flight: the tensor-product LGL
+//             derivative, one pass per axis with one thread per (line, field)
+//             -- the BFAM_KRON_IXIXA / IXAXI / AXIXI contractions of
+//             src/bfam.c:3519-3624 restated per line -- accumulated straight
+//             into A dq + dt rhs in the dq tile;
 //   face    : upwind flux on the gathered traces (conforming faces and the
 //             fine side of hanging faces);
 //   mortar  : faces that go through the glue grid (2:1 hanging faces,
@@ -17,14 +22,11 @@
 //             is interpolated to the four (2D: two) pieces, the flux evaluated
 //             there against each fine neighbour and L2-projected back
 //             (projection[1..2]) -- all pieces of a face at once;
-//   volume  : tensor-product LGL derivative, one pass per axis with one
-//             thread per (line, field), the BFAM_KRON_IXIXA / IXAXI / AXIXI
-//             contractions of src/bfam.c:3519-3624 restated per line, each
-//             value read from shared memory once per axis;
-//   update  : the 2N-storage LSRK stage dq = A dq + dt rhs, q' = q + B dq
-//             (bfamo_lsrk_t, src/bfam.h:1840-1846) in the tail, writing the new
-//             state to the other state buffer so that every element's
-//             neighbours read the stage input unchanged.
+//   update  : lift of the face terms with the lumped LGL mass and the 2N-storage
+//             LSRK stage dq = A dq + dt rhs, q' = q + B dq (bfamo_lsrk_t,
+//             src/bfam.h:1840-1846), writing the new state to the other state
+//             buffer so that every element's neighbours read the stage input
+//             unchanged.
 //
 // State layout in HBM: field-major, element, node (bfam's per-field arrays
 // stacked): q[f * K * Np + e * Np + n], n = i + Nq (j + Nq k).
@@ -37,12 +39,14 @@ namespace bfam_b200
 
 // One axis of the volume operator for one (line, field) work item: the
 // derivative along the line (constant-bank D) and its contributions to the
-// right-hand-side fields, R[c][node] (first axis stores, the others add).
+// right-hand-side fields, accumulated into R = A dq + s rhs (the first axis
+// initialises R from a * dq when rd, from zero otherwise).
 //   rho dv/dt = div S,  dS/dt = lambda div(v) I + mu (grad v + grad v^T)
 template <int DIM, int N, int AXIS>
 __device__ __forceinline__ void volume_axis(const DiffOp<N> &dop,
                                             const double *qs, double *R,
-                                            const ElemData &me, int w)
+                                            const ElemData &me, int w,
+                                            double a, double s, bool rd)
 {
   using S = Shape<DIM, N>;
   constexpr int Nq = S::Nq, Np = S::Np, NL = S::NL;
@@ -63,22 +67,22 @@ __device__ __forceinline__ void volume_axis(const DiffOp<N> &dop,
     base = line;
     stride = Nq * Nq;
   }
-  const double r = AXIS == 0 ? me.rx : (AXIS == 1 ? me.ry : me.rz);
+  const double r = s * (AXIS == 0 ? me.rx : (AXIS == 1 ? me.ry : me.rz));
   // differentiated field per (axis, fsel), bfam field order:
   // 3D x: vx vy vz sxx sxy sxz | y: vx vy vz sxy syy syz | z: vx vy vz sxz syz szz
   // 2D x: vx vy sxx sxy        | y: vx vy sxy syy
   int c;
   if (DIM == 3)
   {
-    const int s = fsel - 3;
+    const int k = fsel - 3;
     if (fsel < 3)
       c = fsel;
     else if (AXIS == 0)
-      c = s == 0 ? 3 : (s == 1 ? 6 : 7);
+      c = k == 0 ? 3 : (k == 1 ? 6 : 7);
     else if (AXIS == 1)
-      c = s == 0 ? 6 : (s == 1 ? 4 : 8);
+      c = k == 0 ? 6 : (k == 1 ? 4 : 8);
     else
-      c = s == 0 ? 7 : (s == 1 ? 8 : 5);
+      c = k == 0 ? 7 : (k == 1 ? 8 : 5);
   }
   else
   {
@@ -97,31 +101,29 @@ __device__ __forceinline__ void volume_axis(const DiffOp<N> &dop,
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
   {
-    double s = 0;
+    double acc = 0;
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      s += dop.D[i + Nq * m] * v[m];
-    dv[i] = r * s;
+      acc += dop.D[i + Nq * m] * v[m];
+    dv[i] = r * acc;
   }
   const double l2m = me.lam + 2 * me.mu;
-  // (target field, coefficient) pairs for this (axis, fsel)
   auto put = [&](int tgt, double coef) {
     double *dst = R + tgt * Np + base;
 #pragma unroll
     for (int i = 0; i < Nq; ++i)
     {
       if (AXIS == 0)
-        dst[i * stride] = coef * dv[i];
+        dst[i * stride] = (rd ? a * dst[i * stride] : 0.0) + coef * dv[i];
       else
         dst[i * stride] += coef * dv[i];
     }
   };
   if (DIM == 3)
   {
-    const int vaxis = AXIS; // velocity component whose normal strain is here
     if (fsel < 3)
     {
-      if (fsel == vaxis)
+      if (fsel == AXIS)
       {
         put(3, AXIS == 0 ? l2m : me.lam);
         put(4, AXIS == 1 ? l2m : me.lam);
@@ -131,22 +133,19 @@ __device__ __forceinline__ void volume_axis(const DiffOp<N> &dop,
       {
         // shear: d v_fsel / d x_AXIS -> S_{fsel,AXIS}
         const int lo = fsel < AXIS ? fsel : AXIS, hi = fsel < AXIS ? AXIS : fsel;
-        const int tgt = (lo == 0 && hi == 1) ? 6 : ((lo == 0) ? 7 : 8);
-        put(tgt, me.mu);
+        put((lo == 0 && hi == 1) ? 6 : ((lo == 0) ? 7 : 8), me.mu);
         if (AXIS == 0 && fsel == 2)
         {
-          // syz gets nothing along x: initialise it here
+          // syz gets nothing along x: start it from A dq here
           double *dst = R + 8 * Np + base;
 #pragma unroll
           for (int i = 0; i < Nq; ++i)
-            dst[i * stride] = 0.0;
+            dst[i * stride] = rd ? a * dst[i * stride] : 0.0;
         }
       }
     }
     else
-    {
       put(fsel - 3, me.irho); // rows of div S -> vx, vy, vz
-    }
   }
   else
   {
@@ -174,25 +173,26 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
                 NFLD = S::NFLD, NJ = S::NJ, NT = S::NT, NPC = S::NPC,
                 ROWS = S::ROWS, NL = S::NL, NDF = S::NDF;
   extern __shared__ __align__(16) double smem[];
-  double *sops = smem;
-  double *qs = sops + S::OPS_PAD;
-  double *dqs = qs + S::SM_QS;
-  double *pt = dqs + S::SM_DQ; // [NF][NFLD][Nfp] plus traces, then jumps
+  double *qs = smem;
+  double *R = qs + S::SM_QS;   // dq tile, becomes A dq + s rhs
+  double *pt = R + S::SM_DQ;   // [NF][NFLD][Nfp] plus traces, then jumps
   double *oi = pt + S::SM_PT;  // [NPC][NFLD][Nfp] own trace on mortar pieces
   double *ms = oi + S::SM_OI;  // [NPC][NFLD][Nfp] fine partners' traces
-  double *R = oi;              // [NFLD][Np] volume rhs, after the mortars
-  double *fcf = pt + S::SM_PT + S::SM_MOR; // [NF][4] face flux constants
-  double *fcp = fcf + 4 * NF;              // [NPC][4] piece flux constants
-  uint64_t *bar = reinterpret_cast<uint64_t *>(fcp + 4 * NPC);
-  const double *sI = sops + Nq * Nq;     // interp[0..2]
-  const double *sP = sops + 4 * Nq * Nq; // proj[0..2]
-  const double *sw = sops + 7 * Nq * Nq;
+  double *fcf = oi + S::SM_MOR; // [NF][4] face flux constants
+  double *fcp = fcf + 4 * NF;   // [NPC][4] piece flux constants
+  double *sIP = fcp + 4 * NPC;  // interp to bottom/top, proj from bottom/top
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sIP + S::SM_IP);
+  const double *sIb = sIP, *sIt = sIP + Nq * Nq;
+  const double *sPb = sIP + 2 * Nq * Nq, *sPt = sIP + 3 * Nq * Nq;
 
   const int e = blockIdx.x;
   const int t = threadIdx.x;
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
-  const bool load_dq = MODE == MODE_STAGE && !sp.first_stage;
+  // R = a dq + s rhs: the stage update (A, dt) or the plain right-hand side
+  const bool rd = MODE == MODE_STAGE && !sp.first_stage;
+  const double a = MODE == MODE_STAGE ? sp.A : 0.0;
+  const double s = MODE == MODE_STAGE ? sp.dt : 1.0;
   const ElemData me = d.ed[e];
   const int2 *desc = d.fdesc + (size_t)e * NF;
 
@@ -222,12 +222,12 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       for (int c = 0; c < NFLD; ++c)
         bulk_g2s(qs + c * Np, d.qin + c * fs + eoff, Np * sizeof(double),
                  &bar[0]);
-      if (S::DQ_SMEM && load_dq)
+      if (rd)
       {
         mbar_expect_tx(&bar[1], NFLD * Np * sizeof(double));
 #pragma unroll
         for (int c = 0; c < NFLD; ++c)
-          bulk_g2s(dqs + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
+          bulk_g2s(R + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
                    &bar[1]);
       }
     }
@@ -237,9 +237,10 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     for (int w = t; w < NFLD * Np; w += NT)
     {
       cp_async8(qs + w, d.qin + (w / Np) * fs + eoff + (w % Np));
-      if (S::DQ_SMEM && load_dq)
-        cp_async8(dqs + w, d.dq + (w / Np) * fs + eoff + (w % Np));
+      if (rd)
+        cp_async8(R + w, d.dq + (w / Np) * fs + eoff + (w % Np));
     }
+    cp_async_commit(); // own state
   }
 
   // neighbour traces of conforming faces and coarse partners of fine-side
@@ -260,9 +261,19 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     for (int c = 0; c < NFLD; ++c)
       cp_async8(dst + c * Nfp, src + c * fs);
     if (pn == 0)
-      face_constants(me, d.ed[ds.x], fcf + 4 * f);
+    {
+      const double *fc = reinterpret_cast<const double *>(d.fcE + (size_t)e * NF + f);
+      cp_async16(fcf + 4 * f, fc);
+      cp_async16(fcf + 4 * f + 2, fc + 2);
+    }
   }
-  cp_async_commit(); // group: q (non-TMA path), dq, face traces
+  // mortar operators: interpolation[1..2], projection[1..2]
+  for (int w = t; w < 4 * Nq * Nq; w += NT)
+  {
+    const int which = w / (Nq * Nq), idx = w % (Nq * Nq);
+    cp_async8(sIP + w, d.ops + (which < 2 ? 2 + which : 3 + which) * Nq * Nq + idx);
+  }
+  cp_async_commit(); // face traces, flux constants, mortar operators
 
   // fine partners of one coarse-side face
   auto issue_coarse = [&](int f) {
@@ -277,7 +288,11 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       for (int c = 0; c < NFLD; ++c)
         cp_async8(dst + c * Nfp, src + c * fs);
       if (pn == 0)
-        face_constants(me, d.ed[gp.x], fcp + 4 * p);
+      {
+        const double *fc = reinterpret_cast<const double *>(d.fcG + g0 + p);
+        cp_async16(fcp + 4 * p, fc);
+        cp_async16(fcp + 4 * p + 2, fc + 2);
+      }
     }
     cp_async_commit();
   };
@@ -287,16 +302,33 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
   else
     cp_async_commit(); // keep the group count uniform
 
-  for (int w = t; w < S::OPS; w += NT)
-    sops[w] = d.ops[w];
-
-  // ------------------------------------------------- phase 1: faces, mortars
+  // ------------------------------- phase 1: volume while the gathers fly
   if constexpr (S::TMA)
   {
     if (!mbar_wait(&bar[0], 0))
       atomicExch(d.err, 1);
+    if (rd && !mbar_wait(&bar[1], 0))
+      atomicExch(d.err, 2);
   }
-  cp_async_wait<1>();
+  else
+  {
+    cp_async_wait<2>(); // own state (face-trace groups may still fly)
+  }
+  __syncthreads();
+  for (int w = t; w < NL * NDF; w += NT)
+    volume_axis<DIM, N, 0>(dop, qs, R, me, w, a, s, rd);
+  __syncthreads();
+  for (int w = t; w < NL * NDF; w += NT)
+    volume_axis<DIM, N, 1>(dop, qs, R, me, w, a, s, rd);
+  if (DIM == 3)
+  {
+    __syncthreads();
+    for (int w = t; w < NL * NDF; w += NT)
+      volume_axis<DIM, N, (DIM == 3 ? 2 : 1)>(dop, qs, R, me, w, a, s, rd);
+  }
+
+  // ------------------------------------------------- phase 2: faces, mortars
+  cp_async_wait<1>(); // face traces
   __syncthreads();
 
   // fine side: coarse partner trace -> my piece, in place (rows, then columns)
@@ -314,9 +346,9 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
         double *x = pt + (f * NFLD + c) * Nfp;
         if (pass == 0)
-          line_apply<N>(sI + (1 + half) * Nq * Nq, x + Nq * line, 1);
+          line_apply<N>(half ? sIt : sIb, x + Nq * line, 1);
         else
-          line_apply<N>(sI + (1 + half) * Nq * Nq, x + line, Nq);
+          line_apply<N>(half ? sIt : sIb, x + line, Nq);
       }
       __syncthreads();
     }
@@ -373,21 +405,15 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const int p = w / (NFLD * ROWS), r = w % (NFLD * ROWS);
       const int c = r / ROWS, line = r % ROWS;
       const int h = (d.gpart[g0 + p].y >> 6) & 7;
-      const double *A = sI + (1 + ((h - 1) & 1)) * Nq * Nq;
-      double v[Nq];
+      double v[Nq], o[Nq];
 #pragma unroll
       for (int i = 0; i < Nq; ++i)
         v[i] = qs[c * Np + gmask<DIM, N>(f, i + Nq * line)];
+      apply_smem<N>(((h - 1) & 1) ? sIt : sIb, v, o);
       double *x = oi + (p * NFLD + c) * Nfp + Nq * line;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-      {
-        double s = 0;
-#pragma unroll
-        for (int i = 0; i < Nq; ++i)
-          s += A[m + Nq * i] * v[i];
-        x[m] = s;
-      }
+        x[m] = o[m];
     }
     __syncthreads();
     if (DIM == 3)
@@ -397,8 +423,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         const int p = w / (NFLD * Nq), r = w % (NFLD * Nq);
         const int c = r / Nq, col = r % Nq;
         const int h = (d.gpart[g0 + p].y >> 6) & 7;
-        line_apply<N>(sI + (1 + ((h - 1) >> 1)) * Nq * Nq,
-                      oi + (p * NFLD + c) * Nfp + col, Nq);
+        line_apply<N>(((h - 1) >> 1) ? sIt : sIb, oi + (p * NFLD + c) * Nfp + col,
+                      Nq);
       }
       __syncthreads();
     }
@@ -431,7 +457,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const int p = w / (NJ * ROWS), r = w % (NJ * ROWS);
       const int c = r / ROWS, line = r % ROWS;
       const int h = (d.gpart[g0 + p].y >> 6) & 7;
-      line_apply<N>(sP + (1 + ((h - 1) & 1)) * Nq * Nq,
+      line_apply<N>(((h - 1) & 1) ? sPt : sPb,
                     oi + (p * NFLD + c) * Nfp + Nq * line, 1);
     }
     __syncthreads();
@@ -442,7 +468,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         const int p = w / (NJ * Nq), r = w % (NJ * Nq);
         const int c = r / Nq, col = r % Nq;
         const int h = (d.gpart[g0 + p].y >> 6) & 7;
-        line_apply<N>(sP + (1 + ((h - 1) >> 1)) * Nq * Nq,
+        line_apply<N>(((h - 1) >> 1) ? sPt : sPb,
                       oi + (p * NFLD + c) * Nfp + col, Nq);
       }
       __syncthreads();
@@ -450,26 +476,12 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     for (int w = t; w < NJ * Nfp; w += NT)
     {
       const int c = w / Nfp, pn = w % Nfp;
-      double s = 0;
+      double sum = 0;
 #pragma unroll
       for (int p = 0; p < NPC; ++p)
-        s += oi[(p * NFLD + c) * Nfp + pn];
-      pt[(f * NFLD + c) * Nfp + pn] = s;
+        sum += oi[(p * NFLD + c) * Nfp + pn];
+      pt[(f * NFLD + c) * Nfp + pn] = sum;
     }
-  }
-  __syncthreads();
-
-  // ------------------------------------------ phase 2: volume, one axis a pass
-  for (int w = t; w < NL * NDF; w += NT)
-    volume_axis<DIM, N, 0>(dop, qs, R, me, w);
-  __syncthreads();
-  for (int w = t; w < NL * NDF; w += NT)
-    volume_axis<DIM, N, 1>(dop, qs, R, me, w);
-  if (DIM == 3)
-  {
-    __syncthreads();
-    for (int w = t; w < NL * NDF; w += NT)
-      volume_axis<DIM, N, (DIM == 3 ? 2 : 1)>(dop, qs, R, me, w);
   }
   __syncthreads();
 
@@ -483,7 +495,6 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       rv[c] = R[c * Np + t];
 
     // lift of the face jump terms with the lumped LGL mass
-    const double iwend = 1.0 / sw[0];
     const double r3[3] = {me.rx, me.ry, me.rz};
 #pragma unroll
     for (int f = 0; f < NF; ++f)
@@ -495,7 +506,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const int pn = DIM == 3 ? (ax == 0 ? j + Nq * k
                                          : (ax == 1 ? i + Nq * k : i + Nq * j))
                               : (ax == 0 ? j : i);
-      const double L = r3[ax] * iwend;
+      const double L = s * r3[ax] * dop.iwend;
       const double sg = side ? 1.0 : -1.0;
       const double *Jf = pt + f * NFLD * Nfp + pn;
       const double dT0 = Jf[0 * Nfp], dT1 = Jf[1 * Nfp];
@@ -530,39 +541,11 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
 
     if constexpr (MODE == MODE_STAGE)
     {
-      double dqo[NFLD];
-      if (load_dq)
-      {
-        if constexpr (S::DQ_SMEM)
-        {
-          if constexpr (S::TMA)
-          {
-            if (!mbar_wait(&bar[1], 0))
-              atomicExch(d.err, 2);
-          }
-#pragma unroll
-          for (int c = 0; c < NFLD; ++c)
-            dqo[c] = dqs[c * Np + t];
-        }
-        else
-        {
-#pragma unroll
-          for (int c = 0; c < NFLD; ++c)
-            dqo[c] = d.dq[c * fs + eoff + t];
-        }
-      }
-      else
-      {
-#pragma unroll
-        for (int c = 0; c < NFLD; ++c)
-          dqo[c] = 0.0;
-      }
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
       {
-        const double dqn = sp.A * dqo[c] + sp.dt * rv[c];
-        d.dq[c * fs + eoff + t] = dqn;
-        d.qout[c * fs + eoff + t] = qs[c * Np + t] + sp.B * dqn;
+        d.dq[c * fs + eoff + t] = rv[c];
+        d.qout[c * fs + eoff + t] = qs[c * Np + t] + sp.B * rv[c];
       }
     }
     else
