@@ -69,7 +69,11 @@ void stage_launch(const DomainView &v, const StageParams &sp,
   constexpr int n2 = (N + 1) * (N + 1);
   DiffOp<N> dop;
   for (int i = 0; i < n2; ++i)
+  {
     dop.D[i] = hops[i];
+    dop.Ib[i] = hops[2 * n2 + i]; // interpolation[1]: refine to bottom
+    dop.Pb[i] = hops[5 * n2 + i]; // projection[1]: coarsen from bottom
+  }
   dop.iwend = 1.0 / hops[7 * n2];
   const size_t smem = (size_t)S::SM_TOTAL * sizeof(double);
   if (mode == MODE_STAGE)
@@ -509,6 +513,24 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
           return fail(BFAM_GPU_EUNSUPPORTED,
                       "non-identity same-level operator (glue order differs "
                       "from the volume order) is not supported");
+  }
+  // the kernels apply the top-half operators as reflections of the
+  // bottom-half ones: A_top(m, i) = A_bot(N - m, N - i)
+  for (int k : {1, 4})
+  {
+    const double *bot = ops.data() + (1 + k) * Nq * Nq;
+    const double *top = ops.data() + (2 + k) * Nq * Nq;
+    double amax = 0;
+    for (int i = 0; i < Nq * Nq; ++i)
+      amax = std::fmax(amax, std::fabs(bot[i]));
+    for (int m = 0; m < Nq; ++m)
+      for (int i = 0; i < Nq; ++i)
+        if (std::fabs(top[m + Nq * i] - bot[(N - m) + Nq * (N - i)]) >
+            1e-13 * (amax > 1 ? amax : 1))
+          return fail(BFAM_GPU_EUNSUPPORTED,
+                      "glue %s operators are not reflections of each other "
+                      "(non-LGL glue grid)",
+                      k == 1 ? "interpolation" : "projection");
   }
   std::memcpy(ops.data() + 7 * Nq * Nq, vol->w, sizeof(double) * Nq);
 

@@ -56,9 +56,15 @@ struct StageParams
 // the FMAs.  All column-major, A(i,m) = A[i + (N+1) m].
 template <int N> struct DiffOp
 {
-  double D[(N + 1) * (N + 1)]; // LGL differentiation
-  double iwend;                // 1 / w_0, the lumped-mass face weight
+  double D[(N + 1) * (N + 1)];  // LGL differentiation
+  double Ib[(N + 1) * (N + 1)]; // interpolation to the bottom half
+  double Pb[(N + 1) * (N + 1)]; // L2 projection from the bottom half
+  double iwend;                 // 1 / w_0, the lumped-mass face weight
 };
+// The top-half operators are the reflections of the bottom-half ones,
+// I_top(m,i) = I_bot(N-m, N-i) and P_top(i,m) = P_bot(N-i, N-m), because the
+// LGL nodes are symmetric (r_{N-i} = -r_i); the host checks this on the glue
+// grid's operators before using it.
 
 enum
 {
@@ -76,6 +82,9 @@ template <int DIM, int N> struct Shape
   // stored jump components: (T* - T-)[0..DIM), (v* - v-)[0..DIM)
   static constexpr int NJ = 2 * DIM;
   static constexpr int NPC = DIM == 3 ? 4 : 2; // mortar pieces per coarse face
+  // trace fields the flux needs on a face normal to axis a: the velocity
+  // and row a of the stress (traction = sg * row a)
+  static constexpr int NTF = 2 * DIM;
   static constexpr int ROWS = DIM == 3 ? Nq : 1; // rows of a face
   static constexpr int NL = Np / Nq;              // lines per direction
   static constexpr int NDF = DIM == 3 ? 6 : 4; // fields differentiated per axis
@@ -91,11 +100,12 @@ template <int DIM, int N> struct Shape
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q
   static constexpr int SM_DQ = SM_QS; // dq, then A dq + dt rhs in place
   static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
-  static constexpr int SM_OI = NPC * NFLD * Nfp + (NPC * NFLD * Nfp) % 2;
+  static constexpr int SM_OI = NPC * NTF * Nfp + (NPC * NTF * Nfp) % 2;
   // mortar scratch: own trace on the pieces, fine partners' traces
   static constexpr int SM_MOR = 2 * SM_OI;
   static constexpr int SM_FC = 4 * (NF + NPC);
-  static constexpr int SM_IP = 4 * Nq * Nq; // interp (bottom, top), proj (.., ..)
+  // differentiation matrix
+  static constexpr int SM_IP = Nq * Nq + (Nq % 2);
   static constexpr int SM_TOTAL =
       SM_QS + SM_DQ + SM_PT + SM_MOR + SM_FC + SM_IP + 4;
 };
@@ -253,10 +263,11 @@ template <int DIM, int N> __device__ __forceinline__ int map_op(int o, int pn)
 // ------------------------------------------------------------- physics
 
 // Jump terms J = (T* - T-, v* - v-) at one face point.  qm/qp hold the
-// point's fields (velocity then stress, bfam field order); n = e_axis * sg is
-// the minus side's outward unit normal.  Upwind: exact Riemann solution of
-// the normal (P, impedance Zp) and tangential (S, impedance Zs) problems;
-// T - Z v travels out of the minus side, T + Z v out of the plus side:
+// point's trace slots (velocity, then row ax of the stress: see trace_field);
+// n = e_axis * sg is the minus side's outward unit normal, so the traction is
+// S n = sg * row ax.  Upwind: exact Riemann solution of the normal (P,
+// impedance Zp) and tangential (S, impedance Zs) problems; T - Z v travels
+// out of the minus side, T + Z v out of the plus side:
 //   v*_n - v-_n = (Zp+ [v_n] + [T_n]) / (Zp- + Zp+),  T*_n - T-_n = Zp- (..)
 //   v*_t - v-_t = (Zs+ [v_t] + [T_t]) / (Zs- + Zs+),  T*_t - T-_t = Zs- (..)
 // fc = {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}, computed once per face.
@@ -267,30 +278,18 @@ __device__ __forceinline__ void flux_jumps(const double *qm, const double *qp,
                                            int flux, double *J)
 {
   double vm[3], vp[3], Tm[3], Tp[3];
-  // traction S n with n = sg e_ax: column ax of S times sg (selects, so the
-  // field arrays stay in registers)
   const bool x = ax == 0, y = ax == 1;
-  if (DIM == 3)
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
   {
-    vm[0] = qm[0]; vm[1] = qm[1]; vm[2] = qm[2];
-    vp[0] = qp[0]; vp[1] = qp[1]; vp[2] = qp[2];
-    Tm[0] = sg * (x ? qm[3] : (y ? qm[6] : qm[7]));
-    Tm[1] = sg * (x ? qm[6] : (y ? qm[4] : qm[8]));
-    Tm[2] = sg * (x ? qm[7] : (y ? qm[8] : qm[5]));
-    Tp[0] = sg * (x ? qp[3] : (y ? qp[6] : qp[7]));
-    Tp[1] = sg * (x ? qp[6] : (y ? qp[4] : qp[8]));
-    Tp[2] = sg * (x ? qp[7] : (y ? qp[8] : qp[5]));
-  }
-  else
-  {
-    vm[0] = qm[0]; vm[1] = qm[1]; vm[2] = 0;
-    vp[0] = qp[0]; vp[1] = qp[1]; vp[2] = 0;
-    Tm[0] = sg * (x ? qm[2] : qm[4]);
-    Tm[1] = sg * (x ? qm[4] : qm[3]);
-    Tm[2] = 0;
-    Tp[0] = sg * (x ? qp[2] : qp[4]);
-    Tp[1] = sg * (x ? qp[4] : qp[3]);
-    Tp[2] = 0;
+    vm[a] = vp[a] = Tm[a] = Tp[a] = 0.0;
+    if (a < DIM)
+    {
+      vm[a] = qm[a];
+      vp[a] = qp[a];
+      Tm[a] = sg * qm[DIM + a];
+      Tp[a] = sg * qp[DIM + a];
+    }
   }
   if (flux == 1)
   {
@@ -338,39 +337,69 @@ template <int DIM> __device__ __forceinline__ constexpr int jslot(int c)
   return c < DIM ? c : 3 + (c - DIM);
 }
 
-// out[m] = sum_i A(m,i) v[i], A column-major in shared memory
-template <int N>
-__device__ __forceinline__ void apply_smem(const double *A, const double *v,
-                                           double *out)
+// out = A v with A the bottom-half mortar operator PROJ ? Pb : Ib of the
+// parameter bank, or its top-half reflection when top != 0:
+//   (A_top v)[m] = (A_bot reverse(v))[N - m].
+template <int N, bool PROJ>
+__device__ __forceinline__ void apply_half(const DiffOp<N> &op, int top,
+                                           const double *v, double *out)
 {
   constexpr int Nq = N + 1;
+  double vr[Nq], o[Nq];
+#pragma unroll
+  for (int i = 0; i < Nq; ++i)
+    vr[i] = top ? v[N - i] : v[i];
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
   {
     double s = 0;
 #pragma unroll
     for (int i = 0; i < Nq; ++i)
-      s += A[m + Nq * i] * v[i];
-    out[m] = s;
+      s += (PROJ ? op.Pb[m + Nq * i] : op.Ib[m + Nq * i]) * vr[i];
+    o[m] = s;
   }
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+    out[m] = top ? o[N - m] : o[m];
 }
 
-// In-place 1-D operator pass on one line of a face array x[m0 + Nq*m1]
-// (stride 1: along face axis 0, stride Nq: along axis 1).  One thread owns
-// one line.
-template <int N>
-__device__ __forceinline__ void line_apply(const double *A, double *x,
-                                           int stride)
+// In-place 1-D mortar operator pass on one line of a face array
+// x[m0 + Nq*m1] (stride 1: along face axis 0, stride Nq: along axis 1).  One
+// thread owns one line.
+template <int N, bool PROJ>
+__device__ __forceinline__ void line_apply(const DiffOp<N> &op, int top,
+                                           double *x, int stride)
 {
   constexpr int Nq = N + 1;
-  double v[Nq], o[Nq];
+  double v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
     v[i] = x[i * stride];
-  apply_smem<N>(A, v, o);
+  apply_half<N, PROJ>(op, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    x[m * stride] = o[m];
+    x[m * stride] = v[m];
+}
+
+// Field of trace slot c on a face normal to axis ax: slots [0, DIM) are the
+// velocity, slots [DIM, 2 DIM) row ax of the stress (bfam field order).
+template <int DIM>
+__device__ __forceinline__ int trace_field(int ax, int c)
+{
+  if (c < DIM)
+    return c;
+  const int k = c - DIM;
+  if (DIM == 3)
+  {
+    if (ax == 0)
+      return k == 0 ? 3 : (k == 1 ? 6 : 7); // sxx sxy sxz
+    if (ax == 1)
+      return k == 0 ? 6 : (k == 1 ? 4 : 8); // sxy syy syz
+    return k == 0 ? 7 : (k == 1 ? 8 : 5);   // sxz syz szz
+  }
+  if (ax == 0)
+    return k == 0 ? 2 : 4; // sxx sxy
+  return k == 0 ? 4 : 3;   // sxy syy
 }
 
 // 16-byte asynchronous copy global -> shared (both 16-byte aligned)

@@ -8,13 +8,9 @@
 //             memory, addressed from a per-face descriptor.  This is the
 //             on-device replacement of vmapP and of the bfam_communicator
 //             ghost exchange (src/bfam.c:6783-6877, 2418-2679);
-//   volume  : while the gathers are in flight: the tensor-product LGL
-//             derivative, one pass per axis with one thread per (line, field)
-//             -- the BFAM_KRON_IXIXA / IXAXI / AXIXI contractions of
-//             src/bfam.c:3519-3624 restated per line -- accumulated straight
-//             into A dq + dt rhs in the dq tile;
 //   face    : upwind flux on the gathered traces (conforming faces and the
-//             fine side of hanging faces);
+//             fine side of hanging faces), lifted with the lumped LGL mass to
+//             per-node field contributions;
 //   mortar  : faces that go through the glue grid (2:1 hanging faces,
 //             src/bfam.c:7328-7520): on the fine side the coarse neighbour's
 //             trace is interpolated to this element's mortar piece
@@ -22,147 +18,24 @@
 //             is interpolated to the four (2D: two) pieces, the flux evaluated
 //             there against each fine neighbour and L2-projected back
 //             (projection[1..2]) -- all pieces of a face at once;
-//   update  : lift of the face terms with the lumped LGL mass and the 2N-storage
-//             LSRK stage dq = A dq + dt rhs, q' = q + B dq (bfamo_lsrk_t,
-//             src/bfam.h:1840-1846), writing the new state to the other state
-//             buffer so that every element's neighbours read the stage input
-//             unchanged.
+//   volume  : one thread per node, the tensor-product LGL derivative along each
+//             axis (the BFAM_KRON_IXIXA / IXAXI / AXIXI contractions of
+//             src/bfam.c:3519-3624 at one node), plus the node's face
+//             contributions;
+//   update  : the 2N-storage LSRK stage dq = A dq + dt rhs, q' = q + B dq
+//             (bfamo_lsrk_t, src/bfam.h:1840-1846), writing the new state to
+//             the other state buffer so that every element's neighbours read
+//             the stage input unchanged.
 //
 // State layout in HBM: field-major, element, node (bfam's per-field arrays
 // stacked): q[f * K * Np + e * Np + n], n = i + Nq (j + Nq k).
 #pragma once
 
 #include "dg_common.cuh"
+#include "dg_volume.cuh"
 
 namespace bfam_b200
 {
-
-// One axis of the volume operator for one (line, field) work item: the
-// derivative along the line (constant-bank D) and its contributions to the
-// right-hand-side fields, accumulated into R = A dq + s rhs (the first axis
-// initialises R from a * dq when rd, from zero otherwise).
-//   rho dv/dt = div S,  dS/dt = lambda div(v) I + mu (grad v + grad v^T)
-template <int DIM, int N, int AXIS>
-__device__ __forceinline__ void volume_axis(const DiffOp<N> &dop,
-                                            const double *qs, double *R,
-                                            const ElemData &me, int w,
-                                            double a, double s, bool rd)
-{
-  using S = Shape<DIM, N>;
-  constexpr int Nq = S::Nq, Np = S::Np, NL = S::NL;
-  const int line = w % NL, fsel = w / NL;
-  int base, stride;
-  if (AXIS == 0)
-  {
-    base = line * Nq;
-    stride = 1;
-  }
-  else if (AXIS == 1)
-  {
-    base = (line % Nq) + Nq * Nq * (line / Nq);
-    stride = Nq;
-  }
-  else
-  {
-    base = line;
-    stride = Nq * Nq;
-  }
-  const double r = s * (AXIS == 0 ? me.rx : (AXIS == 1 ? me.ry : me.rz));
-  // differentiated field per (axis, fsel), bfam field order:
-  // 3D x: vx vy vz sxx sxy sxz | y: vx vy vz sxy syy syz | z: vx vy vz sxz syz szz
-  // 2D x: vx vy sxx sxy        | y: vx vy sxy syy
-  int c;
-  if (DIM == 3)
-  {
-    const int k = fsel - 3;
-    if (fsel < 3)
-      c = fsel;
-    else if (AXIS == 0)
-      c = k == 0 ? 3 : (k == 1 ? 6 : 7);
-    else if (AXIS == 1)
-      c = k == 0 ? 6 : (k == 1 ? 4 : 8);
-    else
-      c = k == 0 ? 7 : (k == 1 ? 8 : 5);
-  }
-  else
-  {
-    if (fsel < 2)
-      c = fsel;
-    else if (AXIS == 0)
-      c = fsel == 2 ? 2 : 4;
-    else
-      c = fsel == 2 ? 4 : 3;
-  }
-  double v[Nq], dv[Nq];
-  const double *src = qs + c * Np + base;
-#pragma unroll
-  for (int m = 0; m < Nq; ++m)
-    v[m] = src[m * stride];
-#pragma unroll
-  for (int i = 0; i < Nq; ++i)
-  {
-    double acc = 0;
-#pragma unroll
-    for (int m = 0; m < Nq; ++m)
-      acc += dop.D[i + Nq * m] * v[m];
-    dv[i] = r * acc;
-  }
-  const double l2m = me.lam + 2 * me.mu;
-  auto put = [&](int tgt, double coef) {
-    double *dst = R + tgt * Np + base;
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-    {
-      if (AXIS == 0)
-        dst[i * stride] = (rd ? a * dst[i * stride] : 0.0) + coef * dv[i];
-      else
-        dst[i * stride] += coef * dv[i];
-    }
-  };
-  if (DIM == 3)
-  {
-    if (fsel < 3)
-    {
-      if (fsel == AXIS)
-      {
-        put(3, AXIS == 0 ? l2m : me.lam);
-        put(4, AXIS == 1 ? l2m : me.lam);
-        put(5, AXIS == 2 ? l2m : me.lam);
-      }
-      else
-      {
-        // shear: d v_fsel / d x_AXIS -> S_{fsel,AXIS}
-        const int lo = fsel < AXIS ? fsel : AXIS, hi = fsel < AXIS ? AXIS : fsel;
-        put((lo == 0 && hi == 1) ? 6 : ((lo == 0) ? 7 : 8), me.mu);
-        if (AXIS == 0 && fsel == 2)
-        {
-          // syz gets nothing along x: start it from A dq here
-          double *dst = R + 8 * Np + base;
-#pragma unroll
-          for (int i = 0; i < Nq; ++i)
-            dst[i * stride] = rd ? a * dst[i * stride] : 0.0;
-        }
-      }
-    }
-    else
-      put(fsel - 3, me.irho); // rows of div S -> vx, vy, vz
-  }
-  else
-  {
-    if (fsel < 2)
-    {
-      if (fsel == AXIS)
-      {
-        put(2, AXIS == 0 ? l2m : me.lam);
-        put(3, AXIS == 1 ? l2m : me.lam);
-      }
-      else
-        put(4, me.mu);
-    }
-    else
-      put(fsel - 2, me.irho);
-  }
-}
 
 template <int DIM, int N, int MODE>
 __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
@@ -171,7 +44,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
   using S = Shape<DIM, N>;
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
                 NFLD = S::NFLD, NJ = S::NJ, NT = S::NT, NPC = S::NPC,
-                ROWS = S::ROWS, NL = S::NL, NDF = S::NDF;
+                ROWS = S::ROWS, NTF = S::NTF;
   extern __shared__ __align__(16) double smem[];
   double *qs = smem;
   double *R = qs + S::SM_QS;   // dq tile, becomes A dq + s rhs
@@ -180,10 +53,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
   double *ms = oi + S::SM_OI;  // [NPC][NFLD][Nfp] fine partners' traces
   double *fcf = oi + S::SM_MOR; // [NF][4] face flux constants
   double *fcp = fcf + 4 * NF;   // [NPC][4] piece flux constants
-  double *sIP = fcp + 4 * NPC;  // interp to bottom/top, proj from bottom/top
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sIP + S::SM_IP);
-  const double *sIb = sIP, *sIt = sIP + Nq * Nq;
-  const double *sPb = sIP + 2 * Nq * Nq, *sPt = sIP + 3 * Nq * Nq;
+  double *sD = fcp + 4 * NPC;   // differentiation matrix
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sD + S::SM_IP);
 
   const int e = blockIdx.x;
   const int t = threadIdx.x;
@@ -258,8 +129,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     const double *src = d.qin + (size_t)ds.x * Np + src_n;
     double *dst = pt + f * NFLD * Nfp + pn;
 #pragma unroll
-    for (int c = 0; c < NFLD; ++c)
-      cp_async8(dst + c * Nfp, src + c * fs);
+    for (int c = 0; c < NTF; ++c)
+      cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
     if (pn == 0)
     {
       const double *fc = reinterpret_cast<const double *>(d.fcE + (size_t)e * NF + f);
@@ -267,13 +138,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       cp_async16(fcf + 4 * f + 2, fc + 2);
     }
   }
-  // mortar operators: interpolation[1..2], projection[1..2]
-  for (int w = t; w < 4 * Nq * Nq; w += NT)
-  {
-    const int which = w / (Nq * Nq), idx = w % (Nq * Nq);
-    cp_async8(sIP + w, d.ops + (which < 2 ? 2 + which : 3 + which) * Nq * Nq + idx);
-  }
-  cp_async_commit(); // face traces, flux constants, mortar operators
+  cp_async_commit(); // face traces, flux constants
 
   // fine partners of one coarse-side face
   auto issue_coarse = [&](int f) {
@@ -283,10 +148,10 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const int p = w / Nfp, pn = w % Nfp;
       const int2 gp = d.gpart[g0 + p];
       const double *src = d.qin + (size_t)gp.x * Np + gmask<DIM, N>(gp.y & 7, pn);
-      double *dst = ms + p * NFLD * Nfp + pn;
+      double *dst = ms + p * NTF * Nfp + pn;
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        cp_async8(dst + c * Nfp, src + c * fs);
+      for (int c = 0; c < NTF; ++c)
+        cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
       if (pn == 0)
       {
         const double *fc = reinterpret_cast<const double *>(d.fcG + g0 + p);
@@ -302,43 +167,31 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
   else
     cp_async_commit(); // keep the group count uniform
 
-  // ------------------------------- phase 1: volume while the gathers fly
+  // differentiation matrix into shared memory (indexed per thread later)
+  for (int w = t; w < Nq * Nq; w += NT)
+    sD[w] = dop.D[w];
+
+  // ------------------------------------------------- phase 1: faces, mortars
   if constexpr (S::TMA)
   {
     if (!mbar_wait(&bar[0], 0))
       atomicExch(d.err, 1);
-    if (rd && !mbar_wait(&bar[1], 0))
-      atomicExch(d.err, 2);
   }
-  else
-  {
-    cp_async_wait<2>(); // own state (face-trace groups may still fly)
-  }
+  cp_async_wait<1>(); // own state (non-TMA path), face traces
   __syncthreads();
-  for (int w = t; w < NL * NDF; w += NT)
-    volume_axis<DIM, N, 0>(dop, qs, R, me, w, a, s, rd);
-  __syncthreads();
-  for (int w = t; w < NL * NDF; w += NT)
-    volume_axis<DIM, N, 1>(dop, qs, R, me, w, a, s, rd);
-  if (DIM == 3)
-  {
-    __syncthreads();
-    for (int w = t; w < NL * NDF; w += NT)
-      volume_axis<DIM, N, (DIM == 3 ? 2 : 1)>(dop, qs, R, me, w, a, s, rd);
-  }
-
-  // ------------------------------------------------- phase 2: faces, mortars
-  cp_async_wait<1>(); // face traces
-  __syncthreads();
+  // lift factor of face axis ax: s (2/h_ax) / w_0
+  const double Lx = s * me.rx * dop.iwend, Ly = s * me.ry * dop.iwend,
+               Lz = s * me.rz * dop.iwend;
+  auto lfac = [&](int ax) { return ax == 0 ? Lx : (ax == 1 ? Ly : Lz); };
 
   // fine side: coarse partner trace -> my piece, in place (rows, then columns)
   if (fine_mask)
   {
     for (int pass = 0; pass < (DIM == 3 ? 2 : 1); ++pass)
     {
-      for (int w = t; w < NF * NFLD * ROWS; w += NT)
+      for (int w = t; w < NF * NTF * ROWS; w += NT)
       {
-        const int f = w / (NFLD * ROWS), r = w % (NFLD * ROWS);
+        const int f = w / (NTF * ROWS), r = w % (NTF * ROWS);
         if (!((fine_mask >> f) & 1))
           continue;
         const int hp = (desc[f].y >> 8) & 7;
@@ -346,17 +199,18 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
         double *x = pt + (f * NFLD + c) * Nfp;
         if (pass == 0)
-          line_apply<N>(half ? sIt : sIb, x + Nq * line, 1);
+          line_apply<N, false>(dop, half, x + Nq * line, 1);
         else
-          line_apply<N>(half ? sIt : sIb, x + line, Nq);
+          line_apply<N, false>(dop, half, x + line, Nq);
       }
       __syncthreads();
     }
   }
 
-  // flux on conforming and fine-side faces: read, barrier, write in place
+  // flux on conforming and fine-side faces, lifted to the face node's field
+  // contributions: read, barrier, write in place
   {
-    double J[6];
+    double lc[NFLD];
     int my_f = -1, my_pn = 0;
     if (t < NF * Nfp)
     {
@@ -369,24 +223,26 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         my_pn = pn;
         const int vm = gmask<DIM, N>(f, pn);
         const int pp = k == 1 ? map_op<DIM, N>((y >> 5) & 7, pn) : pn;
-        double qm[NFLD], qp[NFLD];
+        double qm[NTF], qp[NTF], J[6];
         const double *x = pt + f * NFLD * Nfp;
 #pragma unroll
-        for (int c = 0; c < NFLD; ++c)
+        for (int c = 0; c < NTF; ++c)
         {
-          qm[c] = qs[c * Np + vm];
+          qm[c] = qs[trace_field<DIM>(f >> 1, c) * Np + vm];
           qp[c] = x[c * Nfp + pp];
         }
-        flux_jumps<DIM>(qm, qp, f >> 1, (f & 1) ? 1.0 : -1.0, me.Zp, me.Zs,
-                        fcf + 4 * f, sp.flux, J);
+        const double sg = (f & 1) ? 1.0 : -1.0;
+        flux_jumps<DIM>(qm, qp, f >> 1, sg, me.Zp, me.Zs, fcf + 4 * f, sp.flux,
+                        J);
+        lift_face<DIM>(J, f >> 1, sg, lfac(f >> 1), me, lc);
       }
     }
     __syncthreads();
     if (my_f >= 0)
     {
 #pragma unroll
-      for (int c = 0; c < NJ; ++c)
-        pt[(my_f * NFLD + c) * Nfp + my_pn] = J[jslot<DIM>(c)];
+      for (int c = 0; c < NFLD; ++c)
+        pt[(my_f * NFLD + c) * Nfp + my_pn] = lc[c];
     }
   }
 
@@ -400,31 +256,32 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     cp_async_wait<0>();
     __syncthreads(); // ms holds this face's partners; oi is free
     // own face trace -> pieces, along face axis 0
-    for (int w = t; w < NPC * NFLD * ROWS; w += NT)
+    for (int w = t; w < NPC * NTF * ROWS; w += NT)
     {
-      const int p = w / (NFLD * ROWS), r = w % (NFLD * ROWS);
+      const int p = w / (NTF * ROWS), r = w % (NTF * ROWS);
       const int c = r / ROWS, line = r % ROWS;
       const int h = (d.gpart[g0 + p].y >> 6) & 7;
-      double v[Nq], o[Nq];
+      const double *src = qs + trace_field<DIM>(f >> 1, c) * Np;
+      double v[Nq];
 #pragma unroll
       for (int i = 0; i < Nq; ++i)
-        v[i] = qs[c * Np + gmask<DIM, N>(f, i + Nq * line)];
-      apply_smem<N>(((h - 1) & 1) ? sIt : sIb, v, o);
-      double *x = oi + (p * NFLD + c) * Nfp + Nq * line;
+        v[i] = src[gmask<DIM, N>(f, i + Nq * line)];
+      apply_half<N, false>(dop, (h - 1) & 1, v, v);
+      double *x = oi + (p * NTF + c) * Nfp + Nq * line;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-        x[m] = o[m];
+        x[m] = v[m];
     }
     __syncthreads();
     if (DIM == 3)
     {
-      for (int w = t; w < NPC * NFLD * Nq; w += NT)
+      for (int w = t; w < NPC * NTF * Nq; w += NT)
       {
-        const int p = w / (NFLD * Nq), r = w % (NFLD * Nq);
+        const int p = w / (NTF * Nq), r = w % (NTF * Nq);
         const int c = r / Nq, col = r % Nq;
         const int h = (d.gpart[g0 + p].y >> 6) & 7;
-        line_apply<N>(((h - 1) >> 1) ? sIt : sIb, oi + (p * NFLD + c) * Nfp + col,
-                      Nq);
+        line_apply<N, false>(dop, (h - 1) >> 1, oi + (p * NTF + c) * Nfp + col,
+                             Nq);
       }
       __syncthreads();
     }
@@ -433,11 +290,11 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     {
       const int p = w / Nfp, pn = w % Nfp;
       const int pp = map_op<DIM, N>((d.gpart[g0 + p].y >> 3) & 7, pn);
-      double qm[NFLD], qp[NFLD], J[6];
-      double *x = oi + p * NFLD * Nfp;
-      const double *y = ms + p * NFLD * Nfp;
+      double qm[NTF], qp[NTF], J[6];
+      double *x = oi + p * NTF * Nfp;
+      const double *y = ms + p * NTF * Nfp;
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
+      for (int c = 0; c < NTF; ++c)
       {
         qm[c] = x[c * Nfp + pn];
         qp[c] = y[c * Nfp + pp];
@@ -457,8 +314,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const int p = w / (NJ * ROWS), r = w % (NJ * ROWS);
       const int c = r / ROWS, line = r % ROWS;
       const int h = (d.gpart[g0 + p].y >> 6) & 7;
-      line_apply<N>(((h - 1) & 1) ? sPt : sPb,
-                    oi + (p * NFLD + c) * Nfp + Nq * line, 1);
+      line_apply<N, true>(dop, (h - 1) & 1, oi + (p * NTF + c) * Nfp + Nq * line,
+                          1);
     }
     __syncthreads();
     if (DIM == 3)
@@ -468,34 +325,39 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         const int p = w / (NJ * Nq), r = w % (NJ * Nq);
         const int c = r / Nq, col = r % Nq;
         const int h = (d.gpart[g0 + p].y >> 6) & 7;
-        line_apply<N>(((h - 1) >> 1) ? sPt : sPb,
-                      oi + (p * NFLD + c) * Nfp + col, Nq);
+        line_apply<N, true>(dop, (h - 1) >> 1, oi + (p * NTF + c) * Nfp + col,
+                            Nq);
       }
       __syncthreads();
     }
-    for (int w = t; w < NJ * Nfp; w += NT)
+    for (int pn = t; pn < Nfp; pn += NT)
     {
-      const int c = w / Nfp, pn = w % Nfp;
-      double sum = 0;
+      double J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
-      for (int p = 0; p < NPC; ++p)
-        sum += oi[(p * NFLD + c) * Nfp + pn];
-      pt[(f * NFLD + c) * Nfp + pn] = sum;
+      for (int c = 0; c < NJ; ++c)
+      {
+        double sum = 0;
+#pragma unroll
+        for (int p = 0; p < NPC; ++p)
+          sum += oi[(p * NTF + c) * Nfp + pn];
+        J[jslot<DIM>(c)] = sum;
+      }
+      lift_face<DIM>(J, f >> 1, (f & 1) ? 1.0 : -1.0, lfac(f >> 1), me, lc);
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        pt[(f * NFLD + c) * Nfp + pn] = lc[c];
     }
   }
   __syncthreads();
 
-  // --------------------------------------- phase 3: lift, combine and update
+  // ------------------------ phase 2: volume, face contributions and update
   if (t < Np)
   {
     const int i = t % Nq, j = (t / Nq) % Nq, k = t / (Nq * Nq);
     double rv[NFLD];
-#pragma unroll
-    for (int c = 0; c < NFLD; ++c)
-      rv[c] = R[c * Np + t];
+    volume_node<DIM, N>(qs, sD, me, s, i, j, k, rv);
 
-    // lift of the face jump terms with the lumped LGL mass
-    const double r3[3] = {me.rx, me.ry, me.rz};
+    // lifted face contributions of the faces this node lies on
 #pragma unroll
     for (int f = 0; f < NF; ++f)
     {
@@ -506,41 +368,25 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const int pn = DIM == 3 ? (ax == 0 ? j + Nq * k
                                          : (ax == 1 ? i + Nq * k : i + Nq * j))
                               : (ax == 0 ? j : i);
-      const double L = s * r3[ax] * dop.iwend;
-      const double sg = side ? 1.0 : -1.0;
-      const double *Jf = pt + f * NFLD * Nfp + pn;
-      const double dT0 = Jf[0 * Nfp], dT1 = Jf[1 * Nfp];
-      const double dT2 = DIM == 3 ? Jf[2 * Nfp] : 0.0;
-      const double dv0 = Jf[DIM * Nfp], dv1 = Jf[(DIM + 1) * Nfp];
-      const double dv2 = DIM == 3 ? Jf[5 * Nfp] : 0.0;
-      const double dvv[3] = {dv0, dv1, dv2};
-      const double dvn = sg * dvv[ax];
-      if constexpr (DIM == 3)
-      {
-        rv[0] += L * me.irho * dT0;
-        rv[1] += L * me.irho * dT1;
-        rv[2] += L * me.irho * dT2;
-        const double ll = L * me.lam * dvn, lm = L * me.mu * sg;
-        rv[3] += ll + (ax == 0 ? 2 * lm * dv0 : 0.0);
-        rv[4] += ll + (ax == 1 ? 2 * lm * dv1 : 0.0);
-        rv[5] += ll + (ax == 2 ? 2 * lm * dv2 : 0.0);
-        rv[6] += lm * (ax == 1 ? dv0 : 0.0) + lm * (ax == 0 ? dv1 : 0.0);
-        rv[7] += lm * (ax == 2 ? dv0 : 0.0) + lm * (ax == 0 ? dv2 : 0.0);
-        rv[8] += lm * (ax == 2 ? dv1 : 0.0) + lm * (ax == 1 ? dv2 : 0.0);
-      }
-      else
-      {
-        rv[0] += L * me.irho * dT0;
-        rv[1] += L * me.irho * dT1;
-        const double ll = L * me.lam * dvn, lm = L * me.mu * sg;
-        rv[2] += ll + (ax == 0 ? 2 * lm * dv0 : 0.0);
-        rv[3] += ll + (ax == 1 ? 2 * lm * dv1 : 0.0);
-        rv[4] += lm * (ax == 1 ? dv0 : 0.0) + lm * (ax == 0 ? dv1 : 0.0);
-      }
+      const double *lc = pt + f * NFLD * Nfp + pn;
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        rv[c] += lc[c * Nfp];
     }
 
     if constexpr (MODE == MODE_STAGE)
     {
+      if (rd)
+      {
+        if constexpr (S::TMA)
+        {
+          if (!mbar_wait(&bar[1], 0))
+            atomicExch(d.err, 2);
+        }
+#pragma unroll
+        for (int c = 0; c < NFLD; ++c)
+          rv[c] += a * R[c * Np + t];
+      }
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
       {
