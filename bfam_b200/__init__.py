@@ -113,6 +113,7 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_domain_get_fields": (C.c_int, [vp, P(dp)]),
         "bfam_gpu_domain_rhs": (C.c_int, [vp, P(dp)]),
         "bfam_gpu_domain_energy": (C.c_int, [vp, dp]),
+        "bfam_gpu_domain_energy_noalloc": (C.c_int, [vp, dp]),
         "bfam_gpu_domain_field_device_ptr": (vp, [vp, C.c_int]),
         "bfam_gpu_domain_set_stream": (C.c_int, [vp, vp]),
         "bfam_gpu_domain_sync": (C.c_int, [vp]),
@@ -388,6 +389,13 @@ class GpuDomain:
     def energy(self) -> float:
         e = C.c_double()
         _check(lib().bfam_gpu_domain_energy(self._h, C.byref(e)))
+        return e.value
+
+    def energy_noalloc(self) -> float:
+        """The energy through the entry point that allocates no device memory
+        (fixed scratch compiled into the library; see bfam_gpu.h)."""
+        e = C.c_double()
+        _check(lib().bfam_gpu_domain_energy_noalloc(self._h, C.byref(e)))
         return e.value
 
     def sync(self) -> None:

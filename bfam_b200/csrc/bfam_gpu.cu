@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 using namespace bfam_b200;
@@ -781,6 +782,67 @@ int bfam_gpu_domain_energy(bfam_gpu_domain_t *d, double *energy)
   g_launches.fetch_add(2, std::memory_order_relaxed);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemcpyAsync(energy, d->energy + d->K, sizeof(double),
+                           cudaMemcpyDeviceToHost, d->stream));
+  return bfam_gpu_domain_sync(d);
+}
+
+} // extern "C"
+
+namespace
+{
+
+// Fixed scratch for bfam_gpu_domain_energy_noalloc: one per-element energy
+// slot per element plus the total.  In host code the array's name is only a
+// stand-in; its device address comes from cudaGetSymbolAddress, once per
+// device, and is cached below.
+static __device__ __align__(256) double
+    g_noalloc_energy[BFAM_GPU_NOALLOC_MAX_ELEMENTS + 1];
+
+std::mutex g_noalloc_mu;
+std::vector<double *> g_noalloc_ptr; // indexed by device ordinal
+
+int noalloc_scratch(int device, double **out)
+{
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if ((int)g_noalloc_ptr.size() <= device)
+    g_noalloc_ptr.resize(device + 1, nullptr);
+  if (!g_noalloc_ptr[device])
+  {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_energy);
+    if (e != cudaSuccess || !p)
+      return fail(BFAM_GPU_ECUDA, "cudaGetSymbolAddress(noalloc scratch): %s",
+                  cudaGetErrorString(e));
+    g_noalloc_ptr[device] = static_cast<double *>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int bfam_gpu_domain_energy_noalloc(bfam_gpu_domain_t *d, double *energy)
+{
+  if (!d || !energy)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  if (d->K > BFAM_GPU_NOALLOC_MAX_ELEMENTS)
+    return fail(BFAM_GPU_EINVAL,
+                "domain has %d elements; the allocation-free energy takes at "
+                "most %d (BFAM_GPU_NOALLOC_MAX_ELEMENTS)",
+                d->K, BFAM_GPU_NOALLOC_MAX_ELEMENTS);
+  CUDA_TRY(cudaSetDevice(d->device));
+  double *scratch = nullptr;
+  int rc = noalloc_scratch(d->device, &scratch);
+  if (rc)
+    return rc;
+  d->ks.energy<<<d->K, d->ks.NT, 0, d->stream>>>(d->q[d->cur], d->fs, d->ed,
+                                                 d->ops, scratch);
+  sum_kernel<<<1, 1024, 0, d->stream>>>(scratch, d->K, scratch + d->K);
+  g_launches.fetch_add(2, std::memory_order_relaxed);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(energy, scratch + d->K, sizeof(double),
                            cudaMemcpyDeviceToHost, d->stream));
   return bfam_gpu_domain_sync(d);
 }

@@ -145,6 +145,29 @@ int bfam_gpu_domain_rhs(bfam_gpu_domain_t *dom, double *const *rhs);
 /* Discrete energy sum_e J_e sum_n w_n (rho|v|^2 + S:C^-1:S)/2 (FP64). */
 int bfam_gpu_domain_energy(bfam_gpu_domain_t *dom, double *energy);
 
+/* The same energy, computed without allocating any device memory.  No
+ * counterpart in the reference (bfam has no energy diagnostic on the device).
+ *
+ * For callers that cannot allocate: an application that has handed all of the
+ * device's memory to its own pool (a serving process that commits its whole
+ * HBM budget to admitted solves), or a monitoring hook that runs between time
+ * steps of someone else's solve, where a cudaMalloc can fail or stall.
+ * bfam_gpu_domain_energy allocates its per-element scratch on first use; this
+ * entry point instead uses a fixed scratch array compiled into the library
+ * (BFAM_GPU_NOALLOC_MAX_ELEMENTS + 1 doubles, about 2 MB, held on every GPU
+ * that loads the library until the process exits) and calls no cudaMalloc,
+ * cudaFree or other allocating routine.
+ *
+ * Limits: domains with more than BFAM_GPU_NOALLOC_MAX_ELEMENTS elements are
+ * rejected with BFAM_GPU_EINVAL.  The first call on a device looks up the
+ * array's device address for that device; make that first call before any
+ * stream capture.  All calls in the process share the one array: two calls
+ * whose work overlaps on the GPU (different streams or devices sharing a
+ * context) race and may return wrong values -- serialise them.  Every element
+ * slot is rewritten by each call, so no clearing is needed between calls. */
+#define BFAM_GPU_NOALLOC_MAX_ELEMENTS 262144
+int bfam_gpu_domain_energy_noalloc(bfam_gpu_domain_t *dom, double *energy);
+
 /* Device pointer of field f of the current state (for callers that keep
  * inputs resident and time device work only). */
 double *bfam_gpu_domain_field_device_ptr(bfam_gpu_domain_t *dom, int f);
