@@ -62,59 +62,75 @@ struct KernelSet
 };
 
 // hops: host copy of the operator block Dr | interp[3] | proj[3] | w
-template <int DIM, int N>
+template <int N, typename CT>
+DiffOp<N, CT> make_diffop(const double *hops)
+{
+  constexpr int n2 = (N + 1) * (N + 1);
+  DiffOp<N, CT> dop;
+  for (int i = 0; i < n2; ++i)
+  {
+    dop.D[i] = CT(hops[i]);
+    dop.Ib[i] = CT(hops[2 * n2 + i]); // interpolation[1]: refine to bottom
+    dop.Pb[i] = hops[5 * n2 + i];     // projection[1]: coarsen from bottom
+  }
+  dop.iwend = 1.0 / hops[7 * n2];
+  return dop;
+}
+
+template <int DIM, int N, typename CT>
 void stage_launch(const DomainView &v, const StageParams &sp,
                   const double *hops, int mode, cudaStream_t stream)
 {
   using S = Shape<DIM, N>;
-  constexpr int n2 = (N + 1) * (N + 1);
-  DiffOp<N> dop;
-  for (int i = 0; i < n2; ++i)
-  {
-    dop.D[i] = hops[i];
-    dop.Ib[i] = hops[2 * n2 + i]; // interpolation[1]: refine to bottom
-    dop.Pb[i] = hops[5 * n2 + i]; // projection[1]: coarsen from bottom
-  }
-  dop.iwend = 1.0 / hops[7 * n2];
+  const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
   const size_t smem = (size_t)S::SM_TOTAL * sizeof(double);
   if (mode == MODE_STAGE)
-    dg_stage_kernel<DIM, N, MODE_STAGE><<<v.K, S::NT, smem, stream>>>(v, sp, dop);
+    dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>
+        <<<v.K, S::NT, smem, stream>>>(v, sp, dop);
   else
-    dg_stage_kernel<DIM, N, MODE_RHS><<<v.K, S::NT, smem, stream>>>(v, sp, dop);
+    dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_RHS, CT>
+        <<<v.K, S::NT, smem, stream>>>(v, sp, dop);
 }
 
-template <int DIM, int N> cudaError_t stage_prepare()
+template <typename K> cudaError_t allow_smem(K kernel, int bytes)
+{
+  return cudaFuncSetAttribute((const void *)kernel,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              bytes);
+}
+
+template <int DIM, int N, typename CT> cudaError_t stage_prepare()
 {
   using S = Shape<DIM, N>;
   const int smem = (int)(S::SM_TOTAL * sizeof(double));
-  cudaError_t e = cudaFuncSetAttribute(
-      (const void *)dg_stage_kernel<DIM, N, MODE_STAGE>,
-      cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = allow_smem(
+      dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>, smem);
   if (e != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute((const void *)dg_stage_kernel<DIM, N, MODE_RHS>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              smem);
+  return allow_smem(dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_RHS, CT>,
+                    smem);
 }
 
-template <int DIM, int N> KernelSet make_set()
+template <int DIM, int N, typename CT> KernelSet make_set()
 {
   using S = Shape<DIM, N>;
   KernelSet k;
-  k.launch = stage_launch<DIM, N>;
-  k.prepare = stage_prepare<DIM, N>;
+  k.launch = stage_launch<DIM, N, CT>;
+  k.prepare = stage_prepare<DIM, N, CT>;
   k.energy = dg_energy_kernel<DIM, N>;
   k.NT = S::NT;
   k.smem = (size_t)S::SM_TOTAL * sizeof(double);
   return k;
 }
 
-bool kernel_set(int dim, int N, KernelSet *out)
+// precision: BFAM_GPU_PRECISION_FP64 (double) or _FP32 (float right-hand side)
+bool kernel_set(int dim, int N, int precision, KernelSet *out)
 {
 #define BFAM_CASE(D, NN)                                                       \
   if (dim == D && N == NN)                                                     \
   {                                                                            \
-    *out = make_set<D, NN>();                                                  \
+    *out = precision == BFAM_GPU_PRECISION_FP32 ? make_set<D, NN, float>()     \
+                                                : make_set<D, NN, double>();   \
     return true;                                                               \
   }
   BFAM_CASE(2, 1) BFAM_CASE(2, 2) BFAM_CASE(2, 3) BFAM_CASE(2, 4)
@@ -285,6 +301,7 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double dt,
   sp.first_stage = first;
   sp.flux = d->flux;
   DomainView v = view(d, in);
+  v.dt = dt;
   d->ks.launch(v, sp, d->hops.data(), mode, d->stream);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   CUDA_TRY(cudaGetLastError());
@@ -322,8 +339,11 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
     return fail(BFAM_GPU_EINVAL, "dim must be 2 or 3 (got %d)", dim);
   if (vol->K <= 0)
     return fail(BFAM_GPU_EINVAL, "K must be positive (got %d)", vol->K);
+  if (opts->precision != BFAM_GPU_PRECISION_FP64 &&
+      opts->precision != BFAM_GPU_PRECISION_FP32)
+    return fail(BFAM_GPU_EINVAL, "unknown precision %d", opts->precision);
   KernelSet ks;
-  if (!kernel_set(dim, N, &ks))
+  if (!kernel_set(dim, N, opts->precision, &ks))
     return fail(BFAM_GPU_EUNSUPPORTED, "order N=%d in %dD is not compiled in",
                 N, dim);
   if (!vol->r || !vol->w || !vol->Dr || !vol->vmapM || !vol->vmapP ||
@@ -331,9 +351,6 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
     return fail(BFAM_GPU_EINVAL, "a required volume array is NULL");
   if (opts->flux != BFAM_GPU_FLUX_UPWIND && opts->flux != BFAM_GPU_FLUX_CENTRAL)
     return fail(BFAM_GPU_EINVAL, "unknown flux %d", opts->flux);
-  if (opts->precision != BFAM_GPU_PRECISION_FP64)
-    return fail(BFAM_GPU_EUNSUPPORTED, "precision %d is not available",
-                opts->precision);
 
   const int Nq = N + 1;
   const int Np = dim == 3 ? Nq * Nq * Nq : Nq * Nq;

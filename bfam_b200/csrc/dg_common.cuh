@@ -42,6 +42,7 @@ struct DomainView
   const double4 *__restrict__ fcG; // [Kg] per glue element (coarse side)
   const double *__restrict__ ops;  // Dr | interp[3] | proj[3] | w
   int *err;
+  double dt; // time step of this domain (batches step domains with their own)
 };
 
 struct StageParams
@@ -54,10 +55,12 @@ struct StageParams
 // The 1-D operators travel in the kernel's parameter space so that their
 // entries, indexed by unrolled loop counters, are constant-bank operands of
 // the FMAs.  All column-major, A(i,m) = A[i + (N+1) m].
-template <int N> struct DiffOp
+// CT is the arithmetic type of the right-hand side (double: plain form,
+// float: precision form); the L2 projection always stays in double.
+template <int N, typename CT = double> struct DiffOp
 {
-  double D[(N + 1) * (N + 1)];  // LGL differentiation
-  double Ib[(N + 1) * (N + 1)]; // interpolation to the bottom half
+  CT D[(N + 1) * (N + 1)];      // LGL differentiation
+  CT Ib[(N + 1) * (N + 1)];     // interpolation to the bottom half
   double Pb[(N + 1) * (N + 1)]; // L2 projection from the bottom half
   double iwend;                 // 1 / w_0, the lumped-mass face weight
 };
@@ -103,7 +106,8 @@ template <int DIM, int N> struct Shape
   static constexpr int SM_OI = NPC * NTF * Nfp + (NPC * NTF * Nfp) % 2;
   // mortar scratch: own trace on the pieces, fine partners' traces
   static constexpr int SM_MOR = 2 * SM_OI;
-  static constexpr int SM_FC = 4 * (NF + NPC);
+  // face and piece flux constants, then the element record (ElemData)
+  static constexpr int SM_FC = 4 * (NF + NPC) + 8;
   // differentiation matrix
   static constexpr int SM_IP = Nq * Nq + (Nq % 2);
   static constexpr int SM_TOTAL =
@@ -159,6 +163,13 @@ __device__ __forceinline__ void cp_async_commit()
 template <int NPENDING> __device__ __forceinline__ void cp_async_wait()
 {
   asm volatile("cp.async.wait_group %0;" ::"n"(NPENDING) : "memory");
+}
+
+// Order this CTA's earlier generic-proxy shared-memory accesses (made visible
+// by a preceding __syncthreads) before subsequent async-proxy (TMA) writes.
+__device__ __forceinline__ void fence_proxy_async()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 __device__ __forceinline__ uint64_t global_ns()
@@ -271,18 +282,17 @@ template <int DIM, int N> __device__ __forceinline__ int map_op(int o, int pn)
 //   v*_n - v-_n = (Zp+ [v_n] + [T_n]) / (Zp- + Zp+),  T*_n - T-_n = Zp- (..)
 //   v*_t - v-_t = (Zs+ [v_t] + [T_t]) / (Zs- + Zs+),  T*_t - T-_t = Zs- (..)
 // fc = {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}, computed once per face.
-template <int DIM>
-__device__ __forceinline__ void flux_jumps(const double *qm, const double *qp,
-                                           int ax, double sg, double Zpm,
-                                           double Zsm, const double *fc,
-                                           int flux, double *J)
+template <int DIM, typename CT>
+__device__ __forceinline__ void flux_jumps(const CT *qm, const CT *qp, int ax,
+                                           CT sg, CT Zpm, CT Zsm,
+                                           const double *fc, int flux, CT *J)
 {
-  double vm[3], vp[3], Tm[3], Tp[3];
+  CT vm[3], vp[3], Tm[3], Tp[3];
   const bool x = ax == 0, y = ax == 1;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
   {
-    vm[a] = vp[a] = Tm[a] = Tp[a] = 0.0;
+    vm[a] = vp[a] = Tm[a] = Tp[a] = CT(0);
     if (a < DIM)
     {
       vm[a] = qm[a];
@@ -296,39 +306,31 @@ __device__ __forceinline__ void flux_jumps(const double *qm, const double *qp,
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-      J[a] = 0.5 * (Tp[a] - Tm[a]);
-      J[3 + a] = 0.5 * (vp[a] - vm[a]);
+      J[a] = CT(0.5) * (Tp[a] - Tm[a]);
+      J[3 + a] = CT(0.5) * (vp[a] - vm[a]);
     }
     return;
   }
-  double dv[3], dT[3];
+  CT dv[3], dT[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
   {
     dv[a] = vp[a] - vm[a];
     dT[a] = Tp[a] - Tm[a];
   }
+  const CT f0 = CT(fc[0]), f1 = CT(fc[1]), f2 = CT(fc[2]), f3 = CT(fc[3]);
   // normal parts
-  const double dvn = sg * (x ? dv[0] : (y ? dv[1] : dv[2]));
-  const double dTn = sg * (x ? dT[0] : (y ? dT[1] : dT[2]));
-  const double un = (fc[0] * dvn + dTn) * fc[1];
+  const CT dvn = sg * (x ? dv[0] : (y ? dv[1] : dv[2]));
+  const CT dTn = sg * (x ? dT[0] : (y ? dT[1] : dT[2]));
+  const CT un = (f0 * dvn + dTn) * f1;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
   {
-    const double na = a == ax ? sg : 0.0;
-    const double ut = (fc[2] * (dv[a] - dvn * na) + (dT[a] - dTn * na)) * fc[3];
+    const CT na = a == ax ? sg : CT(0);
+    const CT ut = (f2 * (dv[a] - dvn * na) + (dT[a] - dTn * na)) * f3;
     J[a] = Zpm * un * na + Zsm * ut;
     J[3 + a] = un * na + ut;
   }
-}
-
-__device__ __forceinline__ void face_constants(const ElemData &me,
-                                               const ElemData &ne, double *fc)
-{
-  fc[0] = ne.Zp;
-  fc[1] = 1.0 / (me.Zp + ne.Zp);
-  fc[2] = ne.Zs;
-  fc[3] = 1.0 / (me.Zs + ne.Zs);
 }
 
 // slot in the 6-component jump vector of stored component c
@@ -340,22 +342,23 @@ template <int DIM> __device__ __forceinline__ constexpr int jslot(int c)
 // out = A v with A the bottom-half mortar operator PROJ ? Pb : Ib of the
 // parameter bank, or its top-half reflection when top != 0:
 //   (A_top v)[m] = (A_bot reverse(v))[N - m].
-template <int N, bool PROJ>
-__device__ __forceinline__ void apply_half(const DiffOp<N> &op, int top,
-                                           const double *v, double *out)
+// T is the arithmetic type: CT for interpolations, double for projections.
+template <int N, bool PROJ, typename T, typename CT>
+__device__ __forceinline__ void apply_half(const DiffOp<N, CT> &op, int top,
+                                           const T *v, T *out)
 {
   constexpr int Nq = N + 1;
-  double vr[Nq], o[Nq];
+  T vr[Nq], o[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
     vr[i] = top ? v[N - i] : v[i];
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
   {
-    double s = 0;
+    T s = 0;
 #pragma unroll
     for (int i = 0; i < Nq; ++i)
-      s += (PROJ ? op.Pb[m + Nq * i] : op.Ib[m + Nq * i]) * vr[i];
+      s += (PROJ ? T(op.Pb[m + Nq * i]) : T(op.Ib[m + Nq * i])) * vr[i];
     o[m] = s;
   }
 #pragma unroll
@@ -364,21 +367,21 @@ __device__ __forceinline__ void apply_half(const DiffOp<N> &op, int top,
 }
 
 // In-place 1-D mortar operator pass on one line of a face array
-// x[m0 + Nq*m1] (stride 1: along face axis 0, stride Nq: along axis 1).  One
-// thread owns one line.
-template <int N, bool PROJ>
-__device__ __forceinline__ void line_apply(const DiffOp<N> &op, int top,
+// x[m0 + Nq*m1] (stride 1: along face axis 0, stride Nq: along axis 1),
+// computed in T and stored back in double.  One thread owns one line.
+template <int N, bool PROJ, typename T, typename CT>
+__device__ __forceinline__ void line_apply(const DiffOp<N, CT> &op, int top,
                                            double *x, int stride)
 {
   constexpr int Nq = N + 1;
-  double v[Nq];
+  T v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
-    v[i] = x[i * stride];
-  apply_half<N, PROJ>(op, top, v, v);
+    v[i] = T(x[i * stride]);
+  apply_half<N, PROJ, T, CT>(op, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    x[m * stride] = v[m];
+    x[m * stride] = double(v[m]);
 }
 
 // Field of trace slot c on a face normal to axis ax: slots [0, DIM) are the

@@ -1,13 +1,15 @@
 // Fused DG stage kernel for the isotropic velocity-stress elastic system on
 // affine Cartesian elements (sm_100a).
 //
-// One launch per LSRK stage does, per element (one CTA per element):
+// One element per CTA iteration does:
 //   issue   : every global read of the element is issued up front -- its own
 //             q and dq by TMA bulk copies into shared memory, the neighbours'
 //             face traces by 8-byte cp.async gathers straight into shared
 //             memory, addressed from a per-face descriptor.  This is the
 //             on-device replacement of vmapP and of the bfam_communicator
-//             ghost exchange (src/bfam.c:6783-6877, 2418-2679);
+//             ghost exchange (src/bfam.c:6783-6877, 2418-2679).  Only the six
+//             trace fields the flux uses are gathered (velocity and the stress
+//             row of the face normal);
 //   face    : upwind flux on the gathered traces (conforming faces and the
 //             fine side of hanging faces), lifted with the lumped LGL mass to
 //             per-node field contributions;
@@ -23,9 +25,16 @@
 //             src/bfam.c:3519-3624 at one node), plus the node's face
 //             contributions;
 //   update  : the 2N-storage LSRK stage dq = A dq + dt rhs, q' = q + B dq
-//             (bfamo_lsrk_t, src/bfam.h:1840-1846), writing the new state to
-//             the other state buffer so that every element's neighbours read
-//             the stage input unchanged.
+//             (bfamo_lsrk_t, src/bfam.h:1840-1846) in FP64, writing the new
+//             state to the other state buffer so that every element's
+//             neighbours read the stage input unchanged.
+//
+// Template parameters: NT threads per CTA and MINB CTAs per SM targeted by the
+// register allocation (the tile shape chosen per order), MODE (stage update or
+// right-hand side only) and CT, the arithmetic of the right-hand side (double
+// for the plain form; float for the precision form, where the volume
+// derivative, flux, lift and mortar interpolation run in FP32 while the state,
+// dq, the mortar L2 projection and the update stay FP64).
 //
 // State layout in HBM: field-major, element, node (bfam's per-field arrays
 // stacked): q[f * K * Np + e * Np + n], n = i + Nq (j + Nq k).
@@ -37,44 +46,213 @@
 namespace bfam_b200
 {
 
-template <int DIM, int N, int MODE>
-__global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
-    dg_stage_kernel(DomainView d, StageParams sp, DiffOp<N> dop)
+// Fine partners' traces (the NTF trace fields of face axis ax) and flux
+// constants of one coarse-side glue face, glue elements g0 .. g0 + NPC - 1,
+// gathered into ms / fcp with cp.async (the caller commits the group).
+template <int DIM, int N, int NT>
+__device__ __forceinline__ void
+issue_partners(const double *__restrict__ qin, size_t fs,
+               const int2 *__restrict__ gpart, const double4 *__restrict__ fcG,
+               int g0, int ax, double *ms, double *fcp)
+{
+  using S = Shape<DIM, N>;
+  constexpr int Np = S::Np, Nfp = S::Nfp, NPC = S::NPC, NTF = S::NTF;
+  for (int w = threadIdx.x; w < NPC * Nfp; w += NT)
+  {
+    const int p = w / Nfp, pn = w % Nfp;
+    const int2 gp = gpart[g0 + p];
+    const double *src = qin + (size_t)gp.x * Np + gmask<DIM, N>(gp.y & 7, pn);
+    double *dst = ms + p * NTF * Nfp + pn;
+#pragma unroll
+    for (int c = 0; c < NTF; ++c)
+      cp_async8(dst + c * Nfp, src + trace_field<DIM>(ax, c) * fs);
+    if (pn == 0)
+    {
+      const double *fc = reinterpret_cast<const double *>(fcG + g0 + p);
+      cp_async16(fcp + 4 * p, fc);
+      cp_async16(fcp + 4 * p + 2, fc + 2);
+    }
+  }
+}
+
+// Coarse side of glue face f (glue elements g0 .. g0 + NPC - 1): the
+// element's own trace interpolated to the NPC pieces, the flux against each
+// fine partner there, the jumps L2-projected back (FP64), summed and lifted
+// into pt.  When fnext >= 0 the next coarse face's partners (from gnext) are
+// fetched as soon as ms is free.  Kept out of line: few elements have a
+// coarse face, and inlined its register demand adds to the volume pass's.
+template <int DIM, int N, int NT, typename CT>
+__device__ __noinline__ void
+coarse_face(const double *__restrict__ qin, size_t fs,
+            const int2 *__restrict__ gpart, const double4 *__restrict__ fcG,
+            const DiffOp<N, CT> *dop, int f, int g0, int fnext, int gnext,
+            int flux, double s)
 {
   using S = Shape<DIM, N>;
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
-                NFLD = S::NFLD, NJ = S::NJ, NT = S::NT, NPC = S::NPC,
-                ROWS = S::ROWS, NTF = S::NTF;
+                NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
+                NTF = S::NTF;
   extern __shared__ __align__(16) double smem[];
   double *qs = smem;
-  double *R = qs + S::SM_QS;   // dq tile, becomes A dq + s rhs
-  double *pt = R + S::SM_DQ;   // [NF][NFLD][Nfp] plus traces, then jumps
-  double *oi = pt + S::SM_PT;  // [NPC][NFLD][Nfp] own trace on mortar pieces
-  double *ms = oi + S::SM_OI;  // [NPC][NFLD][Nfp] fine partners' traces
+  double *pt = qs + S::SM_QS + S::SM_DQ;
+  double *oi = pt + S::SM_PT;
+  double *ms = oi + S::SM_OI;
+  double *fcp = oi + S::SM_MOR + 4 * NF;
+  const ElemData &me = *reinterpret_cast<const ElemData *>(fcp + 4 * NPC);
+  const int t = threadIdx.x;
+  auto lfac = [&](int ax) {
+    return CT(s * (ax == 0 ? me.rx : (ax == 1 ? me.ry : me.rz)) * dop->iwend);
+  };
+  cp_async_wait<0>();
+  __syncthreads(); // ms holds this face's partners; oi is free
+  // own face trace -> pieces, along face axis 0
+  for (int w = t; w < NPC * NTF * ROWS; w += NT)
+  {
+    const int p = w / (NTF * ROWS), r = w % (NTF * ROWS);
+    const int c = r / ROWS, line = r % ROWS;
+    const int h = (gpart[g0 + p].y >> 6) & 7;
+    // face line `line` is an arithmetic run of volume nodes
+    const double *src = qs + trace_field<DIM>(f >> 1, c) * Np +
+                        gmask<DIM, N>(f, Nq * line);
+    const int st = gmask<DIM, N>(f, 1) - gmask<DIM, N>(f, 0);
+    CT v[Nq];
+#pragma unroll
+    for (int i = 0; i < Nq; ++i)
+      v[i] = CT(src[st * i]);
+    apply_half<N, false, CT, CT>(*dop, (h - 1) & 1, v, v);
+    double *x = oi + (p * NTF + c) * Nfp + Nq * line;
+#pragma unroll
+    for (int m = 0; m < Nq; ++m)
+      x[m] = double(v[m]);
+  }
+  __syncthreads();
+  if (DIM == 3)
+  {
+    for (int w = t; w < NPC * NTF * Nq; w += NT)
+    {
+      const int p = w / (NTF * Nq), r = w % (NTF * Nq);
+      const int c = r / Nq, col = r % Nq;
+      const int h = (gpart[g0 + p].y >> 6) & 7;
+      line_apply<N, false, CT, CT>(*dop, (h - 1) >> 1,
+                                   oi + (p * NTF + c) * Nfp + col, Nq);
+    }
+    __syncthreads();
+  }
+  // flux on the pieces; jumps overwrite the own trace in place
+  for (int w = t; w < NPC * Nfp; w += NT)
+  {
+    const int p = w / Nfp, pn = w % Nfp;
+    const int pp = map_op<DIM, N>((gpart[g0 + p].y >> 3) & 7, pn);
+    CT qm[NTF], qp[NTF], J[6];
+    double *x = oi + p * NTF * Nfp;
+    const double *y = ms + p * NTF * Nfp;
+#pragma unroll
+    for (int c = 0; c < NTF; ++c)
+    {
+      qm[c] = CT(x[c * Nfp + pn]);
+      qp[c] = CT(y[c * Nfp + pp]);
+    }
+    flux_jumps<DIM, CT>(qm, qp, f >> 1, (f & 1) ? CT(1) : CT(-1), CT(me.Zp),
+                        CT(me.Zs), fcp + 4 * p, flux, J);
+#pragma unroll
+    for (int c = 0; c < NJ; ++c)
+      x[c * Nfp + pn] = double(J[jslot<DIM>(c)]);
+  }
+  __syncthreads(); // ms and fcp free: fetch the next face's partners
+  if (fnext >= 0)
+  {
+    issue_partners<DIM, N, NT>(qin, fs, gpart, fcG, gnext, fnext >> 1, ms,
+                               fcp);
+    cp_async_commit();
+  }
+  // L2 projection back to the coarse face (FP64): axis 0, (axis 1), sum
+  for (int w = t; w < NPC * NJ * ROWS; w += NT)
+  {
+    const int p = w / (NJ * ROWS), r = w % (NJ * ROWS);
+    const int c = r / ROWS, line = r % ROWS;
+    const int h = (gpart[g0 + p].y >> 6) & 7;
+    line_apply<N, true, double, CT>(*dop, (h - 1) & 1,
+                                    oi + (p * NTF + c) * Nfp + Nq * line, 1);
+  }
+  __syncthreads();
+  if (DIM == 3)
+  {
+    for (int w = t; w < NPC * NJ * Nq; w += NT)
+    {
+      const int p = w / (NJ * Nq), r = w % (NJ * Nq);
+      const int c = r / Nq, col = r % Nq;
+      const int h = (gpart[g0 + p].y >> 6) & 7;
+      line_apply<N, true, double, CT>(*dop, (h - 1) >> 1,
+                                      oi + (p * NTF + c) * Nfp + col, Nq);
+    }
+    __syncthreads();
+  }
+  for (int pn = t; pn < Nfp; pn += NT)
+  {
+    CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
+#pragma unroll
+    for (int c = 0; c < NJ; ++c)
+    {
+      double sum = 0;
+#pragma unroll
+      for (int p = 0; p < NPC; ++p)
+        sum += oi[(p * NTF + c) * Nfp + pn];
+      J[jslot<DIM>(c)] = CT(sum);
+    }
+    lift_face<DIM, CT>(J, f >> 1, (f & 1) ? CT(1) : CT(-1), lfac(f >> 1), me,
+                       lc);
+#pragma unroll
+    for (int c = 0; c < NFLD; ++c)
+      pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
+  }
+}
+
+// One element of one stage.  `iter` counts the elements this CTA has done
+// (mbarrier phase parity); the barriers must have been initialised.
+template <int DIM, int N, int NT, int MODE, typename CT>
+__device__ __forceinline__ void stage_element(const DomainView &d,
+                                              const StageParams &sp,
+                                              const DiffOp<N, CT> &dop, int e,
+                                              unsigned iter)
+{
+  using S = Shape<DIM, N>;
+  constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
+                NFLD = S::NFLD, NPC = S::NPC, ROWS = S::ROWS, NTF = S::NTF;
+  static_assert(NT >= NF * Nfp, "one face-node work item per thread");
+  // the dynamic shared array itself (not a pointer parameter), so that all
+  // accesses stay in the shared window with 32-bit addressing
+  extern __shared__ __align__(16) double smem[];
+  double *qs = smem;
+  double *R = qs + S::SM_QS;    // dq tile
+  double *pt = R + S::SM_DQ;    // [NF][NFLD][Nfp] plus traces, then lifted
+  double *oi = pt + S::SM_PT;   // [NPC][NTF][Nfp] own trace on mortar pieces
+  double *ms = oi + S::SM_OI;   // [NPC][NTF][Nfp] fine partners' traces
   double *fcf = oi + S::SM_MOR; // [NF][4] face flux constants
   double *fcp = fcf + 4 * NF;   // [NPC][4] piece flux constants
-  double *sD = fcp + 4 * NPC;   // differentiation matrix
+  double *sE = fcp + 4 * NPC;   // element record
+  double *sD = sE + 8;          // differentiation matrix
   uint64_t *bar = reinterpret_cast<uint64_t *>(sD + S::SM_IP);
 
-  const int e = blockIdx.x;
   const int t = threadIdx.x;
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
-  // R = a dq + s rhs: the stage update (A, dt) or the plain right-hand side
+  const unsigned par = iter & 1u;
+  // the update is dq = a dq + s rhs; the right-hand-side mode uses a = 0, s = 1
   const bool rd = MODE == MODE_STAGE && !sp.first_stage;
   const double a = MODE == MODE_STAGE ? sp.A : 0.0;
-  const double s = MODE == MODE_STAGE ? sp.dt : 1.0;
+  const double s = MODE == MODE_STAGE ? d.dt : 1.0;
   const ElemData me = d.ed[e];
   const int2 *desc = d.fdesc + (size_t)e * NF;
 
-  int kinds = 0, coarse_mask = 0, fine_mask = 0;
+  int coarse_mask = 0, fine_mask = 0;
+  bool permuted = false; // a glue face whose partner nodes are permuted
 #pragma unroll
   for (int f = 0; f < NF; ++f)
   {
-    const int k = desc[f].y & 3;
-    kinds |= k << (2 * f);
-    coarse_mask |= (k == 2) << f;
-    fine_mask |= (k == 1 && ((desc[f].y >> 8) & 7) != 0) << f;
+    const int y = desc[f].y;
+    coarse_mask |= ((y & 3) == 2) << f;
+    fine_mask |= ((y & 3) == 1 && ((y >> 8) & 7) != 0) << f;
+    permuted |= (y & 3) == 1 && ((y >> 5) & 7) != 0;
   }
 
   // ---------------------------------------------------------- phase 0: issue
@@ -82,12 +260,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
   {
     if (t == 0)
     {
-      mbar_init(&bar[0], 1);
-      mbar_init(&bar[1], 1);
-    }
-    __syncthreads();
-    if (t == 0)
-    {
+      fence_proxy_async(); // shared memory of the previous element is free
       mbar_expect_tx(&bar[0], NFLD * Np * sizeof(double));
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
@@ -111,8 +284,8 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       if (rd)
         cp_async8(R + w, d.dq + (w / Np) * fs + eoff + (w % Np));
     }
-    cp_async_commit(); // own state
   }
+  cp_async_commit(); // own state (non-TMA path)
 
   // neighbour traces of conforming faces and coarse partners of fine-side
   // glue faces, gathered into pt in this element's face-node order
@@ -124,8 +297,9 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     if (k == 2)
       continue;
     const int nface = (ds.y >> 2) & 7;
-    const int src_n = k == 0 ? gmask<DIM, N>(nface, face_perm<DIM, N>((ds.y >> 5) & 7, pn))
-                             : gmask<DIM, N>(nface, pn);
+    const int src_n =
+        k == 0 ? gmask<DIM, N>(nface, face_perm<DIM, N>((ds.y >> 5) & 7, pn))
+               : gmask<DIM, N>(nface, pn);
     const double *src = d.qin + (size_t)ds.x * Np + src_n;
     double *dst = pt + f * NFLD * Nfp + pn;
 #pragma unroll
@@ -133,56 +307,39 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
     if (pn == 0)
     {
-      const double *fc = reinterpret_cast<const double *>(d.fcE + (size_t)e * NF + f);
+      const double *fc =
+          reinterpret_cast<const double *>(d.fcE + (size_t)e * NF + f);
       cp_async16(fcf + 4 * f, fc);
       cp_async16(fcf + 4 * f + 2, fc + 2);
     }
   }
-  cp_async_commit(); // face traces, flux constants
+  if (t < 4)
+    cp_async16(sE + 2 * t,
+               reinterpret_cast<const double *>(d.ed + e) + 2 * t);
+  cp_async_commit(); // face traces, flux constants, element record
 
-  // fine partners of one coarse-side face
-  auto issue_coarse = [&](int f) {
-    const int32_t g0 = desc[f].x;
-    for (int w = t; w < NPC * Nfp; w += NT)
-    {
-      const int p = w / Nfp, pn = w % Nfp;
-      const int2 gp = d.gpart[g0 + p];
-      const double *src = d.qin + (size_t)gp.x * Np + gmask<DIM, N>(gp.y & 7, pn);
-      double *dst = ms + p * NTF * Nfp + pn;
-#pragma unroll
-      for (int c = 0; c < NTF; ++c)
-        cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
-      if (pn == 0)
-      {
-        const double *fc = reinterpret_cast<const double *>(d.fcG + g0 + p);
-        cp_async16(fcp + 4 * p, fc);
-        cp_async16(fcp + 4 * p + 2, fc + 2);
-      }
-    }
-    cp_async_commit();
-  };
   int next_coarse = coarse_mask ? __ffs(coarse_mask) - 1 : -1;
   if (next_coarse >= 0)
-    issue_coarse(next_coarse);
-  else
-    cp_async_commit(); // keep the group count uniform
+    issue_partners<DIM, N, NT>(d.qin, fs, d.gpart, d.fcG, desc[next_coarse].x,
+                               next_coarse >> 1, ms, fcp);
+  cp_async_commit(); // fine partners (possibly empty)
 
   // differentiation matrix into shared memory (indexed per thread later)
   for (int w = t; w < Nq * Nq; w += NT)
-    sD[w] = dop.D[w];
+    sD[w] = double(dop.D[w]);
 
   // ------------------------------------------------- phase 1: faces, mortars
   if constexpr (S::TMA)
   {
-    if (!mbar_wait(&bar[0], 0))
+    if (!mbar_wait(&bar[0], par))
       atomicExch(d.err, 1);
   }
   cp_async_wait<1>(); // own state (non-TMA path), face traces
   __syncthreads();
   // lift factor of face axis ax: s (2/h_ax) / w_0
-  const double Lx = s * me.rx * dop.iwend, Ly = s * me.ry * dop.iwend,
-               Lz = s * me.rz * dop.iwend;
-  auto lfac = [&](int ax) { return ax == 0 ? Lx : (ax == 1 ? Ly : Lz); };
+  auto lfac = [&](int ax) {
+    return CT(s * (ax == 0 ? me.rx : (ax == 1 ? me.ry : me.rz)) * dop.iwend);
+  };
 
   // fine side: coarse partner trace -> my piece, in place (rows, then columns)
   if (fine_mask)
@@ -199,18 +356,20 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
         double *x = pt + (f * NFLD + c) * Nfp;
         if (pass == 0)
-          line_apply<N, false>(dop, half, x + Nq * line, 1);
+          line_apply<N, false, CT, CT>(dop, half, x + Nq * line, 1);
         else
-          line_apply<N, false>(dop, half, x + line, Nq);
+          line_apply<N, false, CT, CT>(dop, half, x + line, Nq);
       }
       __syncthreads();
     }
   }
 
   // flux on conforming and fine-side faces, lifted to the face node's field
-  // contributions: read, barrier, write in place
+  // contributions, written in place over the node's own trace slots.  A
+  // thread reads only its own node's slots unless a glue face permutes its
+  // partner's nodes; only then are all reads finished before any write.
   {
-    double lc[NFLD];
+    CT lc[NFLD];
     int my_f = -1, my_pn = 0;
     if (t < NF * Nfp)
     {
@@ -223,26 +382,35 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
         my_pn = pn;
         const int vm = gmask<DIM, N>(f, pn);
         const int pp = k == 1 ? map_op<DIM, N>((y >> 5) & 7, pn) : pn;
-        double qm[NTF], qp[NTF], J[6];
+        CT qm[NTF], qp[NTF], J[6];
         const double *x = pt + f * NFLD * Nfp;
 #pragma unroll
         for (int c = 0; c < NTF; ++c)
         {
-          qm[c] = qs[trace_field<DIM>(f >> 1, c) * Np + vm];
-          qp[c] = x[c * Nfp + pp];
+          qm[c] = CT(qs[trace_field<DIM>(f >> 1, c) * Np + vm]);
+          qp[c] = CT(x[c * Nfp + pp]);
         }
-        const double sg = (f & 1) ? 1.0 : -1.0;
-        flux_jumps<DIM>(qm, qp, f >> 1, sg, me.Zp, me.Zs, fcf + 4 * f, sp.flux,
-                        J);
-        lift_face<DIM>(J, f >> 1, sg, lfac(f >> 1), me, lc);
+        const CT sg = (f & 1) ? CT(1) : CT(-1);
+        flux_jumps<DIM, CT>(qm, qp, f >> 1, sg, CT(me.Zp), CT(me.Zs),
+                            fcf + 4 * f, sp.flux, J);
+        lift_face<DIM, CT>(J, f >> 1, sg, lfac(f >> 1), me, lc);
+        if (!permuted)
+        {
+#pragma unroll
+          for (int c = 0; c < NFLD; ++c)
+            pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
+        }
       }
     }
-    __syncthreads();
-    if (my_f >= 0)
+    if (permuted)
     {
+      __syncthreads();
+      if (my_f >= 0)
+      {
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        pt[(my_f * NFLD + c) * Nfp + my_pn] = lc[c];
+        for (int c = 0; c < NFLD; ++c)
+          pt[(my_f * NFLD + c) * Nfp + my_pn] = double(lc[c]);
+      }
     }
   }
 
@@ -252,110 +420,43 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
     const int f = next_coarse;
     coarse_mask &= ~(1 << f);
     next_coarse = coarse_mask ? __ffs(coarse_mask) - 1 : -1;
-    const int32_t g0 = desc[f].x;
-    cp_async_wait<0>();
-    __syncthreads(); // ms holds this face's partners; oi is free
-    // own face trace -> pieces, along face axis 0
-    for (int w = t; w < NPC * NTF * ROWS; w += NT)
-    {
-      const int p = w / (NTF * ROWS), r = w % (NTF * ROWS);
-      const int c = r / ROWS, line = r % ROWS;
-      const int h = (d.gpart[g0 + p].y >> 6) & 7;
-      const double *src = qs + trace_field<DIM>(f >> 1, c) * Np;
-      double v[Nq];
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        v[i] = src[gmask<DIM, N>(f, i + Nq * line)];
-      apply_half<N, false>(dop, (h - 1) & 1, v, v);
-      double *x = oi + (p * NTF + c) * Nfp + Nq * line;
-#pragma unroll
-      for (int m = 0; m < Nq; ++m)
-        x[m] = v[m];
-    }
-    __syncthreads();
-    if (DIM == 3)
-    {
-      for (int w = t; w < NPC * NTF * Nq; w += NT)
-      {
-        const int p = w / (NTF * Nq), r = w % (NTF * Nq);
-        const int c = r / Nq, col = r % Nq;
-        const int h = (d.gpart[g0 + p].y >> 6) & 7;
-        line_apply<N, false>(dop, (h - 1) >> 1, oi + (p * NTF + c) * Nfp + col,
-                             Nq);
-      }
-      __syncthreads();
-    }
-    // flux on the pieces; jumps overwrite the own trace in place
-    for (int w = t; w < NPC * Nfp; w += NT)
-    {
-      const int p = w / Nfp, pn = w % Nfp;
-      const int pp = map_op<DIM, N>((d.gpart[g0 + p].y >> 3) & 7, pn);
-      double qm[NTF], qp[NTF], J[6];
-      double *x = oi + p * NTF * Nfp;
-      const double *y = ms + p * NTF * Nfp;
-#pragma unroll
-      for (int c = 0; c < NTF; ++c)
-      {
-        qm[c] = x[c * Nfp + pn];
-        qp[c] = y[c * Nfp + pp];
-      }
-      flux_jumps<DIM>(qm, qp, f >> 1, (f & 1) ? 1.0 : -1.0, me.Zp, me.Zs,
-                      fcp + 4 * p, sp.flux, J);
-#pragma unroll
-      for (int c = 0; c < NJ; ++c)
-        x[c * Nfp + pn] = J[jslot<DIM>(c)];
-    }
-    __syncthreads(); // ms and fcp free: fetch the next face's partners
-    if (next_coarse >= 0)
-      issue_coarse(next_coarse);
-    // L2 projection back to the coarse face: axis 0, (axis 1), sum of pieces
-    for (int w = t; w < NPC * NJ * ROWS; w += NT)
-    {
-      const int p = w / (NJ * ROWS), r = w % (NJ * ROWS);
-      const int c = r / ROWS, line = r % ROWS;
-      const int h = (d.gpart[g0 + p].y >> 6) & 7;
-      line_apply<N, true>(dop, (h - 1) & 1, oi + (p * NTF + c) * Nfp + Nq * line,
-                          1);
-    }
-    __syncthreads();
-    if (DIM == 3)
-    {
-      for (int w = t; w < NPC * NJ * Nq; w += NT)
-      {
-        const int p = w / (NJ * Nq), r = w % (NJ * Nq);
-        const int c = r / Nq, col = r % Nq;
-        const int h = (d.gpart[g0 + p].y >> 6) & 7;
-        line_apply<N, true>(dop, (h - 1) >> 1, oi + (p * NTF + c) * Nfp + col,
-                            Nq);
-      }
-      __syncthreads();
-    }
-    for (int pn = t; pn < Nfp; pn += NT)
-    {
-      double J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
-#pragma unroll
-      for (int c = 0; c < NJ; ++c)
-      {
-        double sum = 0;
-#pragma unroll
-        for (int p = 0; p < NPC; ++p)
-          sum += oi[(p * NTF + c) * Nfp + pn];
-        J[jslot<DIM>(c)] = sum;
-      }
-      lift_face<DIM>(J, f >> 1, (f & 1) ? 1.0 : -1.0, lfac(f >> 1), me, lc);
-#pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        pt[(f * NFLD + c) * Nfp + pn] = lc[c];
-    }
+    coarse_face<DIM, N, NT, CT>(d.qin, fs, d.gpart, d.fcG, &dop, f, desc[f].x,
+                                next_coarse,
+                                next_coarse >= 0 ? desc[next_coarse].x : 0,
+                                sp.flux, s);
   }
   __syncthreads();
 
   // ------------------------ phase 2: volume, face contributions and update
-  if (t < Np)
+  if (MODE == MODE_STAGE && rd)
   {
-    const int i = t % Nq, j = (t / Nq) % Nq, k = t / (Nq * Nq);
-    double rv[NFLD];
-    volume_node<DIM, N>(qs, sD, me, s, i, j, k, rv);
+    if constexpr (S::TMA)
+    {
+      if (!mbar_wait(&bar[1], par))
+        atomicExch(d.err, 2);
+    }
+  }
+  constexpr int NODE_ITERS = (Np + NT - 1) / NT;
+#pragma unroll 1
+  for (int it = 0; it < NODE_ITERS; ++it)
+  {
+    const int n = t + it * NT;
+    if (n >= Np)
+      break;
+    const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
+    double acc[NFLD];
+    if constexpr (sizeof(CT) == sizeof(double))
+    {
+      volume_node<DIM, N, CT>(qs, sD, me, s, i, j, k, acc);
+    }
+    else
+    {
+      CT rv[NFLD];
+      volume_node<DIM, N, CT>(qs, sD, me, s, i, j, k, rv);
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        acc[c] = double(rv[c]);
+    }
 
     // lifted face contributions of the faces this node lies on
 #pragma unroll
@@ -371,35 +472,79 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT, Shape<DIM, N>::MINB)
       const double *lc = pt + f * NFLD * Nfp + pn;
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
-        rv[c] += lc[c * Nfp];
+        acc[c] += lc[c * Nfp];
     }
 
     if constexpr (MODE == MODE_STAGE)
     {
       if (rd)
       {
-        if constexpr (S::TMA)
-        {
-          if (!mbar_wait(&bar[1], 0))
-            atomicExch(d.err, 2);
-        }
 #pragma unroll
         for (int c = 0; c < NFLD; ++c)
-          rv[c] += a * R[c * Np + t];
+          acc[c] += a * R[c * Np + n];
       }
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
       {
-        d.dq[c * fs + eoff + t] = rv[c];
-        d.qout[c * fs + eoff + t] = qs[c * Np + t] + sp.B * rv[c];
+        d.dq[c * fs + eoff + n] = acc[c];
+        d.qout[c * fs + eoff + n] = qs[c * Np + n] + sp.B * acc[c];
       }
     }
     else
     {
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
-        d.rhs[c * fs + eoff + t] = rv[c];
+        d.rhs[c * fs + eoff + n] = acc[c];
     }
+  }
+}
+
+__device__ __forceinline__ void stage_barriers_init(int offset)
+{
+  extern __shared__ __align__(16) double smem[];
+  if (threadIdx.x == 0)
+  {
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + offset);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+  }
+  __syncthreads();
+}
+
+template <int DIM, int N> __host__ __device__ constexpr int bar_offset()
+{
+  using S = Shape<DIM, N>;
+  return S::SM_QS + S::SM_DQ + S::SM_PT + S::SM_MOR + S::SM_FC + S::SM_IP;
+}
+
+// One domain, one element per CTA.
+template <int DIM, int N, int NT, int MINB, int MODE, typename CT>
+__global__ void __launch_bounds__(NT, MINB)
+    dg_stage_kernel(DomainView d, StageParams sp,
+                    const __grid_constant__ DiffOp<N, CT> dop)
+{
+  stage_barriers_init(bar_offset<DIM, N>());
+  stage_element<DIM, N, NT, MODE, CT>(d, sp, dop, blockIdx.x, 0);
+}
+
+// Many domains of the same order in one persistent launch: CTAs stride over
+// a flat work list of (domain, element) pairs, each domain with its own
+// arrays and time step.
+template <int DIM, int N, int NT, int MINB, int MODE, typename CT>
+__global__ void __launch_bounds__(NT, MINB)
+    dg_stage_batch_kernel(const DomainView *__restrict__ views,
+                          const int2 *__restrict__ work, int nwork,
+                          StageParams sp,
+                          const __grid_constant__ DiffOp<N, CT> dop)
+{
+  stage_barriers_init(bar_offset<DIM, N>());
+  unsigned iter = 0;
+  for (int i = blockIdx.x; i < nwork; i += gridDim.x, ++iter)
+  {
+    const int2 w = work[i];
+    const DomainView d = views[w.x];
+    stage_element<DIM, N, NT, MODE, CT>(d, sp, dop, w.y, iter);
+    __syncthreads(); // shared memory is reused by the next element
   }
 }
 

@@ -1,4 +1,6 @@
-// Volume term and face lift of the elastic DG operator, per node.
+// Volume term and face lift of the elastic DG operator, per node.  CT is the
+// arithmetic type (double: plain form, float: precision form); the state in
+// shared memory is always double.
 #pragma once
 
 #include "dg_common.cuh"
@@ -13,21 +15,22 @@ namespace bfam_b200
 // contractions of src/bfam.c:3519-3624 evaluated at one node.  sD is the
 // column-major D(i,m) = sD[i + Nq m] in shared memory; lines along x are
 // read with 16-byte loads when Nq is even.
-template <int DIM, int N>
+template <int DIM, int N, typename CT>
 __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
                                             const ElemData &me, double s, int i,
-                                            int j, int k, double *rv)
+                                            int j, int k, CT *rv)
 {
   using S = Shape<DIM, N>;
   constexpr int Nq = S::Nq, Np = S::Np, NFLD = S::NFLD;
-  const double l2m = me.lam + 2 * me.mu;
+  const CT lam = CT(me.lam), mu = CT(me.mu), irho = CT(me.irho);
+  const CT l2m = lam + CT(2) * mu;
 #pragma unroll
   for (int c = 0; c < NFLD; ++c)
-    rv[c] = 0.0;
+    rv[c] = CT(0);
 
   // derivative of field c along axis ax at this node
-  auto deriv = [&](int c, int ax, const double *Dl) {
-    double acc = 0;
+  auto deriv = [&](int c, int ax, const CT *Dl) {
+    CT acc = 0;
     if (ax == 0)
     {
       const double *x = qs + c * Np + Nq * (j + Nq * k);
@@ -37,15 +40,15 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
         for (int m = 0; m < Nq; m += 2)
         {
           const double2 v = *reinterpret_cast<const double2 *>(x + m);
-          acc += Dl[m] * v.x;
-          acc += Dl[m + 1] * v.y;
+          acc += Dl[m] * CT(v.x);
+          acc += Dl[m + 1] * CT(v.y);
         }
       }
       else
       {
 #pragma unroll
         for (int m = 0; m < Nq; ++m)
-          acc += Dl[m] * x[m];
+          acc += Dl[m] * CT(x[m]);
       }
     }
     else if (ax == 1)
@@ -53,73 +56,73 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
       const double *x = qs + c * Np + i + Nq * Nq * k;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-        acc += Dl[m] * x[Nq * m];
+        acc += Dl[m] * CT(x[Nq * m]);
     }
     else
     {
       const double *x = qs + c * Np + i + Nq * j;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-        acc += Dl[m] * x[Nq * Nq * m];
+        acc += Dl[m] * CT(x[Nq * Nq * m]);
     }
     return acc;
   };
 
-  double Dl[Nq];
+  CT Dl[Nq];
   // x
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = sD[i + Nq * m];
-    const double r = s * me.rx;
-    const double dvx = r * deriv(0, 0, Dl), dvy = r * deriv(1, 0, Dl);
+      Dl[m] = CT(sD[i + Nq * m]);
+    const CT r = CT(s * me.rx);
+    const CT dvx = r * deriv(0, 0, Dl), dvy = r * deriv(1, 0, Dl);
     if (DIM == 3)
     {
-      const double dvz = r * deriv(2, 0, Dl);
+      const CT dvz = r * deriv(2, 0, Dl);
       rv[3] += l2m * dvx;
-      rv[4] += me.lam * dvx;
-      rv[5] += me.lam * dvx;
-      rv[6] += me.mu * dvy;
-      rv[7] += me.mu * dvz;
-      rv[0] += me.irho * r * deriv(3, 0, Dl); // sxx
-      rv[1] += me.irho * r * deriv(6, 0, Dl); // sxy
-      rv[2] += me.irho * r * deriv(7, 0, Dl); // sxz
+      rv[4] += lam * dvx;
+      rv[5] += lam * dvx;
+      rv[6] += mu * dvy;
+      rv[7] += mu * dvz;
+      rv[0] += irho * r * deriv(3, 0, Dl); // sxx
+      rv[1] += irho * r * deriv(6, 0, Dl); // sxy
+      rv[2] += irho * r * deriv(7, 0, Dl); // sxz
     }
     else
     {
       rv[2] += l2m * dvx;
-      rv[3] += me.lam * dvx;
-      rv[4] += me.mu * dvy;
-      rv[0] += me.irho * r * deriv(2, 0, Dl); // sxx
-      rv[1] += me.irho * r * deriv(4, 0, Dl); // sxy
+      rv[3] += lam * dvx;
+      rv[4] += mu * dvy;
+      rv[0] += irho * r * deriv(2, 0, Dl); // sxx
+      rv[1] += irho * r * deriv(4, 0, Dl); // sxy
     }
   }
   // y
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = sD[j + Nq * m];
-    const double r = s * me.ry;
-    const double dvx = r * deriv(0, 1, Dl), dvy = r * deriv(1, 1, Dl);
+      Dl[m] = CT(sD[j + Nq * m]);
+    const CT r = CT(s * me.ry);
+    const CT dvx = r * deriv(0, 1, Dl), dvy = r * deriv(1, 1, Dl);
     if (DIM == 3)
     {
-      const double dvz = r * deriv(2, 1, Dl);
-      rv[6] += me.mu * dvx;
-      rv[3] += me.lam * dvy;
+      const CT dvz = r * deriv(2, 1, Dl);
+      rv[6] += mu * dvx;
+      rv[3] += lam * dvy;
       rv[4] += l2m * dvy;
-      rv[5] += me.lam * dvy;
-      rv[8] += me.mu * dvz;
-      rv[0] += me.irho * r * deriv(6, 1, Dl); // sxy
-      rv[1] += me.irho * r * deriv(4, 1, Dl); // syy
-      rv[2] += me.irho * r * deriv(8, 1, Dl); // syz
+      rv[5] += lam * dvy;
+      rv[8] += mu * dvz;
+      rv[0] += irho * r * deriv(6, 1, Dl); // sxy
+      rv[1] += irho * r * deriv(4, 1, Dl); // syy
+      rv[2] += irho * r * deriv(8, 1, Dl); // syz
     }
     else
     {
-      rv[4] += me.mu * dvx;
-      rv[2] += me.lam * dvy;
+      rv[4] += mu * dvx;
+      rv[2] += lam * dvy;
       rv[3] += l2m * dvy;
-      rv[0] += me.irho * r * deriv(4, 1, Dl); // sxy
-      rv[1] += me.irho * r * deriv(3, 1, Dl); // syy
+      rv[0] += irho * r * deriv(4, 1, Dl); // sxy
+      rv[1] += irho * r * deriv(3, 1, Dl); // syy
     }
   }
   // z
@@ -127,18 +130,18 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = sD[k + Nq * m];
-    const double r = s * me.rz;
-    const double dvx = r * deriv(0, 2, Dl), dvy = r * deriv(1, 2, Dl),
-                 dvz = r * deriv(2, 2, Dl);
-    rv[7] += me.mu * dvx;
-    rv[8] += me.mu * dvy;
-    rv[3] += me.lam * dvz;
-    rv[4] += me.lam * dvz;
+      Dl[m] = CT(sD[k + Nq * m]);
+    const CT r = CT(s * me.rz);
+    const CT dvx = r * deriv(0, 2, Dl), dvy = r * deriv(1, 2, Dl),
+             dvz = r * deriv(2, 2, Dl);
+    rv[7] += mu * dvx;
+    rv[8] += mu * dvy;
+    rv[3] += lam * dvz;
+    rv[4] += lam * dvz;
     rv[5] += l2m * dvz;
-    rv[0] += me.irho * r * deriv(7, 2, Dl); // sxz
-    rv[1] += me.irho * r * deriv(8, 2, Dl); // syz
-    rv[2] += me.irho * r * deriv(5, 2, Dl); // szz
+    rv[0] += irho * r * deriv(7, 2, Dl); // sxz
+    rv[1] += irho * r * deriv(8, 2, Dl); // syz
+    rv[2] += irho * r * deriv(5, 2, Dl); // szz
   }
 }
 
@@ -147,34 +150,35 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
 // mapped onto the fields (outward normal n = sg e_ax):
 //   v += L / rho (T* - T-),
 //   S += L (lambda (dv.n) I + mu (dv n^T + n dv^T)).
-template <int DIM>
-__device__ __forceinline__ void lift_face(const double *J, int ax, double sg,
-                                          double L, const ElemData &me,
-                                          double *out)
+template <int DIM, typename CT>
+__device__ __forceinline__ void lift_face(const CT *J, int ax, CT sg, CT L,
+                                          const ElemData &me, CT *out)
 {
   const bool x = ax == 0, y = ax == 1, z = ax == 2;
-  const double dv0 = J[3], dv1 = J[4], dv2 = J[5];
-  const double dvn = sg * (x ? dv0 : (y ? dv1 : dv2));
-  const double Li = L * me.irho, ll = L * me.lam * dvn, lm = L * me.mu * sg;
+  const CT dv0 = J[3], dv1 = J[4], dv2 = J[5];
+  const CT dvn = sg * (x ? dv0 : (y ? dv1 : dv2));
+  const CT Li = L * CT(me.irho), ll = L * CT(me.lam) * dvn,
+           lm = L * CT(me.mu) * sg;
+  const CT two = CT(2), zero = CT(0);
   if (DIM == 3)
   {
     out[0] = Li * J[0];
     out[1] = Li * J[1];
     out[2] = Li * J[2];
-    out[3] = ll + (x ? 2 * lm * dv0 : 0.0);
-    out[4] = ll + (y ? 2 * lm * dv1 : 0.0);
-    out[5] = ll + (z ? 2 * lm * dv2 : 0.0);
-    out[6] = lm * ((y ? dv0 : 0.0) + (x ? dv1 : 0.0));
-    out[7] = lm * ((z ? dv0 : 0.0) + (x ? dv2 : 0.0));
-    out[8] = lm * ((z ? dv1 : 0.0) + (y ? dv2 : 0.0));
+    out[3] = ll + (x ? two * lm * dv0 : zero);
+    out[4] = ll + (y ? two * lm * dv1 : zero);
+    out[5] = ll + (z ? two * lm * dv2 : zero);
+    out[6] = lm * ((y ? dv0 : zero) + (x ? dv1 : zero));
+    out[7] = lm * ((z ? dv0 : zero) + (x ? dv2 : zero));
+    out[8] = lm * ((z ? dv1 : zero) + (y ? dv2 : zero));
   }
   else
   {
     out[0] = Li * J[0];
     out[1] = Li * J[1];
-    out[2] = ll + (x ? 2 * lm * dv0 : 0.0);
-    out[3] = ll + (y ? 2 * lm * dv1 : 0.0);
-    out[4] = lm * ((y ? dv0 : 0.0) + (x ? dv1 : 0.0));
+    out[2] = ll + (x ? two * lm * dv0 : zero);
+    out[3] = ll + (y ? two * lm * dv1 : zero);
+    out[4] = lm * ((y ? dv0 : zero) + (x ? dv1 : zero));
   }
 }
 
