@@ -83,7 +83,7 @@ void stage_launch(const DomainView &v, const StageParams &sp,
 {
   using S = Shape<DIM, N>;
   const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
-  const size_t smem = (size_t)S::SM_TOTAL * sizeof(double);
+  const size_t smem = stage_smem_bytes<DIM, N, CT>();
   if (mode == MODE_STAGE)
     dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>
         <<<v.K, S::NT, smem, stream>>>(v, sp, dop);
@@ -102,7 +102,7 @@ template <typename K> cudaError_t allow_smem(K kernel, int bytes)
 template <int DIM, int N, typename CT> cudaError_t stage_prepare()
 {
   using S = Shape<DIM, N>;
-  const int smem = (int)(S::SM_TOTAL * sizeof(double));
+  const int smem = (int)stage_smem_bytes<DIM, N, CT>();
   cudaError_t e = allow_smem(
       dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>, smem);
   if (e != cudaSuccess)
@@ -119,7 +119,7 @@ template <int DIM, int N, typename CT> KernelSet make_set()
   k.prepare = stage_prepare<DIM, N, CT>;
   k.energy = dg_energy_kernel<DIM, N>;
   k.NT = S::NT;
-  k.smem = (size_t)S::SM_TOTAL * sizeof(double);
+  k.smem = stage_smem_bytes<DIM, N, CT>();
   return k;
 }
 

@@ -112,6 +112,9 @@ template <int DIM, int N> struct Shape
   static constexpr int SM_IP = Nq * Nq + (Nq % 2);
   static constexpr int SM_TOTAL =
       SM_QS + SM_DQ + SM_PT + SM_MOR + SM_FC + SM_IP + 4;
+  // precision form only: FP32 copy of q minus the element's first node,
+  // after the mbarriers
+  static constexpr int SM_QF = (NFLD * Np + 3) / 4 * 2;
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -273,50 +276,40 @@ template <int DIM, int N> __device__ __forceinline__ int map_op(int o, int pn)
 
 // ------------------------------------------------------------- physics
 
-// Jump terms J = (T* - T-, v* - v-) at one face point.  qm/qp hold the
-// point's trace slots (velocity, then row ax of the stress: see trace_field);
-// n = e_axis * sg is the minus side's outward unit normal, so the traction is
-// S n = sg * row ax.  Upwind: exact Riemann solution of the normal (P,
-// impedance Zp) and tangential (S, impedance Zs) problems; T - Z v travels
-// out of the minus side, T + Z v out of the plus side:
+// Jump terms J = (T* - T-, v* - v-) at one face point from the trace jumps
+// dq = q+ - q- of the point's trace slots (velocity, then row ax of the
+// stress: see trace_field), formed in FP64 by the caller so that the
+// precision form rounds the jump, not the traces.  n = e_axis * sg is the
+// minus side's outward unit normal, so the traction jump is sg * [row ax].
+// Upwind: exact Riemann solution of the normal (P, impedance Zp) and
+// tangential (S, impedance Zs) problems; T - Z v travels out of the minus
+// side, T + Z v out of the plus side:
 //   v*_n - v-_n = (Zp+ [v_n] + [T_n]) / (Zp- + Zp+),  T*_n - T-_n = Zp- (..)
 //   v*_t - v-_t = (Zs+ [v_t] + [T_t]) / (Zs- + Zs+),  T*_t - T-_t = Zs- (..)
-// fc = {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}, computed once per face.
+// Central: half the jumps.  fc = {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)},
+// computed once per face.
 template <int DIM, typename CT>
-__device__ __forceinline__ void flux_jumps(const CT *qm, const CT *qp, int ax,
-                                           CT sg, CT Zpm, CT Zsm,
-                                           const double *fc, int flux, CT *J)
+__device__ __forceinline__ void flux_jumps(const CT *dq, int ax, CT sg,
+                                           CT Zpm, CT Zsm, const double *fc,
+                                           int flux, CT *J)
 {
-  CT vm[3], vp[3], Tm[3], Tp[3];
   const bool x = ax == 0, y = ax == 1;
+  CT dv[3], dT[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
   {
-    vm[a] = vp[a] = Tm[a] = Tp[a] = CT(0);
-    if (a < DIM)
-    {
-      vm[a] = qm[a];
-      vp[a] = qp[a];
-      Tm[a] = sg * qm[DIM + a];
-      Tp[a] = sg * qp[DIM + a];
-    }
+    dv[a] = a < DIM ? dq[a] : CT(0);
+    dT[a] = a < DIM ? sg * dq[DIM + a] : CT(0);
   }
   if (flux == 1)
   {
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-      J[a] = CT(0.5) * (Tp[a] - Tm[a]);
-      J[3 + a] = CT(0.5) * (vp[a] - vm[a]);
+      J[a] = CT(0.5) * dT[a];
+      J[3 + a] = CT(0.5) * dv[a];
     }
     return;
-  }
-  CT dv[3], dT[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-  {
-    dv[a] = vp[a] - vm[a];
-    dT[a] = Tp[a] - Tm[a];
   }
   const CT f0 = CT(fc[0]), f1 = CT(fc[1]), f2 = CT(fc[2]), f3 = CT(fc[3]);
   // normal parts
@@ -368,20 +361,26 @@ __device__ __forceinline__ void apply_half(const DiffOp<N, CT> &op, int top,
 
 // In-place 1-D mortar operator pass on one line of a face array
 // x[m0 + Nq*m1] (stride 1: along face axis 0, stride Nq: along axis 1),
-// computed in T and stored back in double.  One thread owns one line.
+// computed in T and stored back in double.  One thread owns one line.  An
+// interpolation in a type narrower than double is applied to the line minus
+// its first value, which is added back in double (interpolation reproduces
+// constants), so that the rounding is relative to the variation along the
+// line rather than to the values.
 template <int N, bool PROJ, typename T, typename CT>
 __device__ __forceinline__ void line_apply(const DiffOp<N, CT> &op, int top,
                                            double *x, int stride)
 {
   constexpr int Nq = N + 1;
+  constexpr bool OFFSET = !PROJ && sizeof(T) < sizeof(double);
+  const double ref = OFFSET ? x[0] : 0.0;
   T v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
-    v[i] = T(x[i * stride]);
+    v[i] = OFFSET ? T(x[i * stride] - ref) : T(x[i * stride]);
   apply_half<N, PROJ, T, CT>(op, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    x[m * stride] = double(v[m]);
+    x[m * stride] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
 // Field of trace slot c on a face normal to axis ax: slots [0, DIM) are the

@@ -115,15 +115,18 @@ coarse_face(const double *__restrict__ qin, size_t fs,
     const double *src = qs + trace_field<DIM>(f >> 1, c) * Np +
                         gmask<DIM, N>(f, Nq * line);
     const int st = gmask<DIM, N>(f, 1) - gmask<DIM, N>(f, 0);
+    // narrower than double: interpolate the variation along the line
+    constexpr bool OFFSET = sizeof(CT) < sizeof(double);
+    const double ref = OFFSET ? src[0] : 0.0;
     CT v[Nq];
 #pragma unroll
     for (int i = 0; i < Nq; ++i)
-      v[i] = CT(src[st * i]);
+      v[i] = OFFSET ? CT(src[st * i] - ref) : CT(src[st * i]);
     apply_half<N, false, CT, CT>(*dop, (h - 1) & 1, v, v);
     double *x = oi + (p * NTF + c) * Nfp + Nq * line;
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      x[m] = double(v[m]);
+      x[m] = OFFSET ? ref + double(v[m]) : double(v[m]);
   }
   __syncthreads();
   if (DIM == 3)
@@ -143,16 +146,13 @@ coarse_face(const double *__restrict__ qin, size_t fs,
   {
     const int p = w / Nfp, pn = w % Nfp;
     const int pp = map_op<DIM, N>((gpart[g0 + p].y >> 3) & 7, pn);
-    CT qm[NTF], qp[NTF], J[6];
+    CT dq[NTF], J[6];
     double *x = oi + p * NTF * Nfp;
     const double *y = ms + p * NTF * Nfp;
 #pragma unroll
     for (int c = 0; c < NTF; ++c)
-    {
-      qm[c] = CT(x[c * Nfp + pn]);
-      qp[c] = CT(y[c * Nfp + pp]);
-    }
-    flux_jumps<DIM, CT>(qm, qp, f >> 1, (f & 1) ? CT(1) : CT(-1), CT(me.Zp),
+      dq[c] = CT(y[c * Nfp + pp] - x[c * Nfp + pn]);
+    flux_jumps<DIM, CT>(dq, f >> 1, (f & 1) ? CT(1) : CT(-1), CT(me.Zp),
                         CT(me.Zs), fcp + 4 * p, flux, J);
 #pragma unroll
     for (int c = 0; c < NJ; ++c)
@@ -230,8 +230,18 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   double *fcf = oi + S::SM_MOR; // [NF][4] face flux constants
   double *fcp = fcf + 4 * NF;   // [NPC][4] piece flux constants
   double *sE = fcp + 4 * NPC;   // element record
-  double *sD = sE + 8;          // differentiation matrix
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sD + S::SM_IP);
+  CT *sD = reinterpret_cast<CT *>(sE + 8); // differentiation matrix
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sE + 8 + S::SM_IP);
+  // the volume pass's copy of q: q itself in the plain form; in the
+  // precision form FP32 q minus the element's first node per field (the
+  // derivative of a constant is zero), so that rounding is relative to the
+  // variation inside the element
+  constexpr bool NARROW = sizeof(CT) < sizeof(double);
+  CT *qv;
+  if constexpr (NARROW)
+    qv = reinterpret_cast<CT *>(smem + S::SM_TOTAL);
+  else
+    qv = qs;
 
   const int t = threadIdx.x;
   const size_t fs = d.fs;
@@ -326,7 +336,7 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
 
   // differentiation matrix into shared memory (indexed per thread later)
   for (int w = t; w < Nq * Nq; w += NT)
-    sD[w] = double(dop.D[w]);
+    sD[w] = dop.D[w];
 
   // ------------------------------------------------- phase 1: faces, mortars
   if constexpr (S::TMA)
@@ -335,6 +345,13 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
       atomicExch(d.err, 1);
   }
   cp_async_wait<1>(); // own state (non-TMA path), face traces
+  if constexpr (NARROW && !S::TMA)
+    __syncthreads(); // other threads' cp.async writes of q
+  if constexpr (NARROW)
+  {
+    for (int w = t; w < NFLD * Np; w += NT)
+      qv[w] = CT(qs[w] - qs[(w / Np) * Np]);
+  }
   __syncthreads();
   // lift factor of face axis ax: s (2/h_ax) / w_0
   auto lfac = [&](int ax) {
@@ -382,16 +399,13 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
         my_pn = pn;
         const int vm = gmask<DIM, N>(f, pn);
         const int pp = k == 1 ? map_op<DIM, N>((y >> 5) & 7, pn) : pn;
-        CT qm[NTF], qp[NTF], J[6];
+        CT dq[NTF], J[6];
         const double *x = pt + f * NFLD * Nfp;
 #pragma unroll
         for (int c = 0; c < NTF; ++c)
-        {
-          qm[c] = CT(qs[trace_field<DIM>(f >> 1, c) * Np + vm]);
-          qp[c] = CT(x[c * Nfp + pp]);
-        }
+          dq[c] = CT(x[c * Nfp + pp] - qs[trace_field<DIM>(f >> 1, c) * Np + vm]);
         const CT sg = (f & 1) ? CT(1) : CT(-1);
-        flux_jumps<DIM, CT>(qm, qp, f >> 1, sg, CT(me.Zp), CT(me.Zs),
+        flux_jumps<DIM, CT>(dq, f >> 1, sg, CT(me.Zp), CT(me.Zs),
                             fcf + 4 * f, sp.flux, J);
         lift_face<DIM, CT>(J, f >> 1, sg, lfac(f >> 1), me, lc);
         if (!permuted)
@@ -445,14 +459,14 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
       break;
     const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
     double acc[NFLD];
-    if constexpr (sizeof(CT) == sizeof(double))
+    if constexpr (!NARROW)
     {
-      volume_node<DIM, N, CT>(qs, sD, me, s, i, j, k, acc);
+      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
     }
     else
     {
       CT rv[NFLD];
-      volume_node<DIM, N, CT>(qs, sD, me, s, i, j, k, rv);
+      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
         acc[c] = double(rv[c]);
@@ -515,6 +529,15 @@ template <int DIM, int N> __host__ __device__ constexpr int bar_offset()
 {
   using S = Shape<DIM, N>;
   return S::SM_QS + S::SM_DQ + S::SM_PT + S::SM_MOR + S::SM_FC + S::SM_IP;
+}
+
+// dynamic shared memory of one CTA of the stage kernel
+template <int DIM, int N, typename CT>
+__host__ __device__ constexpr size_t stage_smem_bytes()
+{
+  using S = Shape<DIM, N>;
+  return (S::SM_TOTAL + (sizeof(CT) < sizeof(double) ? S::SM_QF : 0)) *
+         sizeof(double);
 }
 
 // One domain, one element per CTA.

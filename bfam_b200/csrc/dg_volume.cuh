@@ -3,6 +3,8 @@
 // shared memory is always double.
 #pragma once
 
+#include <type_traits>
+
 #include "dg_common.cuh"
 
 namespace bfam_b200
@@ -12,11 +14,12 @@ namespace bfam_b200
 //   rho dv/dt = div S,  dS/dt = lambda div(v) I + mu (grad v + grad v^T)
 // with the derivative along each axis the 1-D LGL differentiation matrix
 // applied along that axis -- the BFAM_KRON_IXIXA / IXAXI / AXIXI
-// contractions of src/bfam.c:3519-3624 evaluated at one node.  sD is the
-// column-major D(i,m) = sD[i + Nq m] in shared memory; lines along x are
-// read with 16-byte loads when Nq is even.
+// contractions of src/bfam.c:3519-3624 evaluated at one node.  qs is the
+// element's state tile in CT, sD the column-major D(i,m) = sD[i + Nq m], both
+// in shared memory; lines along x are read with vector loads (2 doubles, or
+// 4 or 2 floats) where Nq allows.
 template <int DIM, int N, typename CT>
-__device__ __forceinline__ void volume_node(const double *qs, const double *sD,
+__device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
                                             const ElemData &me, double s, int i,
                                             int j, int k, CT *rv)
 {
@@ -33,37 +36,52 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
     CT acc = 0;
     if (ax == 0)
     {
-      const double *x = qs + c * Np + Nq * (j + Nq * k);
-      if constexpr (Nq % 2 == 0)
+      const CT *x = qs + c * Np + Nq * (j + Nq * k);
+      constexpr bool F4 = sizeof(CT) == 4 && Nq % 4 == 0;
+      if constexpr (F4)
       {
+#pragma unroll
+        for (int m = 0; m < Nq; m += 4)
+        {
+          const float4 v = *reinterpret_cast<const float4 *>(x + m);
+          acc += Dl[m] * v.x;
+          acc += Dl[m + 1] * v.y;
+          acc += Dl[m + 2] * v.z;
+          acc += Dl[m + 3] * v.w;
+        }
+      }
+      else if constexpr (Nq % 2 == 0)
+      {
+        using V2 = typename std::conditional<sizeof(CT) == 4, float2,
+                                             double2>::type;
 #pragma unroll
         for (int m = 0; m < Nq; m += 2)
         {
-          const double2 v = *reinterpret_cast<const double2 *>(x + m);
-          acc += Dl[m] * CT(v.x);
-          acc += Dl[m + 1] * CT(v.y);
+          const V2 v = *reinterpret_cast<const V2 *>(x + m);
+          acc += Dl[m] * v.x;
+          acc += Dl[m + 1] * v.y;
         }
       }
       else
       {
 #pragma unroll
         for (int m = 0; m < Nq; ++m)
-          acc += Dl[m] * CT(x[m]);
+          acc += Dl[m] * x[m];
       }
     }
     else if (ax == 1)
     {
-      const double *x = qs + c * Np + i + Nq * Nq * k;
+      const CT *x = qs + c * Np + i + Nq * Nq * k;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-        acc += Dl[m] * CT(x[Nq * m]);
+        acc += Dl[m] * x[Nq * m];
     }
     else
     {
-      const double *x = qs + c * Np + i + Nq * j;
+      const CT *x = qs + c * Np + i + Nq * j;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-        acc += Dl[m] * CT(x[Nq * Nq * m]);
+        acc += Dl[m] * x[Nq * Nq * m];
     }
     return acc;
   };
@@ -73,7 +91,7 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = CT(sD[i + Nq * m]);
+      Dl[m] = sD[i + Nq * m];
     const CT r = CT(s * me.rx);
     const CT dvx = r * deriv(0, 0, Dl), dvy = r * deriv(1, 0, Dl);
     if (DIM == 3)
@@ -101,7 +119,7 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = CT(sD[j + Nq * m]);
+      Dl[m] = sD[j + Nq * m];
     const CT r = CT(s * me.ry);
     const CT dvx = r * deriv(0, 1, Dl), dvy = r * deriv(1, 1, Dl);
     if (DIM == 3)
@@ -130,7 +148,7 @@ __device__ __forceinline__ void volume_node(const double *qs, const double *sD,
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = CT(sD[k + Nq * m]);
+      Dl[m] = sD[k + Nq * m];
     const CT r = CT(s * me.rz);
     const CT dvx = r * deriv(0, 2, Dl), dvy = r * deriv(1, 2, Dl),
              dvz = r * deriv(2, 2, Dl);

@@ -92,7 +92,10 @@ class Oracle:
 
     def __del__(self):
         if getattr(self, "_h", None):
-            lib().oracle_free(self._h)
+            try:
+                lib().oracle_free(self._h)
+            except (TypeError, AttributeError):  # interpreter shutdown
+                pass
             self._h = None
 
     def rhs(self, q: np.ndarray, nthreads: int = 0) -> np.ndarray:
