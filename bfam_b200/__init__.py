@@ -20,6 +20,9 @@ FIELDS_2D = ("vx", "vy", "sxx", "syy", "sxy")
 FIELDS_3D = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
 
 FLUX_UPWIND, FLUX_CENTRAL = 0, 1
+# status codes of the C-ABI
+(BFAM_GPU_EINVAL, BFAM_GPU_ENOMEM, BFAM_GPU_ECUDA, BFAM_GPU_ETIMEOUT,
+ BFAM_GPU_EUNSUPPORTED) = (-1, -2, -3, -4, -5)
 PRECISION_FP64, PRECISION_FP32 = 0, 1
 LSRK_KC54, LSRK_FE, LSRK_HEUN, LSRK_W33 = 0, 1, 2, 3
 
@@ -80,6 +83,11 @@ class GlueDesc(C.Structure):
                 ("interpolation", dp * 3), ("projection", dp * 3)]
 
 
+class SourceDesc(C.Structure):
+    _fields_ = [("x", C.c_double * 3), ("force", C.c_double * 3),
+                ("f0", C.c_double), ("t0", C.c_double)]
+
+
 class Options(C.Structure):
     _fields_ = [("flux", C.c_int), ("precision", C.c_int),
                 ("mem_budget_bytes", C.c_size_t), ("device", C.c_int)]
@@ -121,6 +129,22 @@ def _declare(L: C.CDLL) -> None:
         "bfam_ts_lsrk_step": (C.c_int, [vp, C.c_double, C.c_int, C.c_int]),
         "bfam_ts_lsrk_time": (C.c_int, [vp, dp]),
         "bfam_ts_lsrk_free": (C.c_int, [vp]),
+        "bfam_gpu_domain_set_source": (C.c_int, [vp, P(SourceDesc)]),
+        "bfam_gpu_domain_set_receivers": (C.c_int, [vp, C.c_int, dp, C.c_int]),
+        "bfam_gpu_domain_get_seismograms": (C.c_int, [vp, dp, P(C.c_int)]),
+        "bfam_gpu_batch_create": (C.c_int, [P(vp), C.c_int, C.c_int, dp, P(vp)]),
+        "bfam_gpu_batch_set_stream": (C.c_int, [vp, vp]),
+        "bfam_gpu_batch_step": (C.c_int, [vp, dp, C.c_int, C.c_int]),
+        "bfam_gpu_batch_time": (C.c_int, [vp, C.c_int, dp]),
+        "bfam_gpu_batch_sync": (C.c_int, [vp]),
+        "bfam_gpu_batch_free": (C.c_int, [vp]),
+        "bfam_gpu_batch_num_groups": (C.c_int, [vp]),
+        "bfam_gpu_batch_group_info": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int),
+                                                P(C.c_int), P(C.c_int64)]),
+        "bfam_gpu_tile_count": (C.c_int, [C.c_int, C.c_int]),
+        "bfam_gpu_tile_shape": (C.c_int, [C.c_int, C.c_int, C.c_int, P(C.c_int),
+                                          P(C.c_int)]),
+        "bfam_gpu_batch_set_tile": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "bfam_gpu_launch_count": (C.c_uint64, []),
         "bfam_gpu_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
     }
@@ -406,6 +430,103 @@ class GpuDomain:
 
     def set_stream(self, stream_ptr: int) -> None:
         _check(lib().bfam_gpu_domain_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def set_source(self, x, force, f0: float, t0: float) -> None:
+        """Ricker point force f(t) F at x (bfam_gpu_domain_set_source)."""
+        s = SourceDesc()
+        for a in range(3):
+            s.x[a] = x[a] if a < len(x) else 0.0
+            s.force[a] = force[a] if a < len(force) else 0.0
+        s.f0, s.t0 = f0, t0
+        _check(lib().bfam_gpu_domain_set_source(self._h, C.byref(s)))
+
+    def clear_source(self) -> None:
+        _check(lib().bfam_gpu_domain_set_source(self._h, None))
+
+    def set_receivers(self, x: np.ndarray, max_samples: int) -> None:
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, 3))
+        self._nrecv = len(x)
+        _check(lib().bfam_gpu_domain_set_receivers(self._h, len(x), _dp(x), max_samples))
+        self._max_samples = max_samples
+
+    def seismograms(self) -> np.ndarray:
+        """samples [nsamples][nrecv][nfields]"""
+        nr = getattr(self, "_nrecv", 0)
+        out = np.empty((max(getattr(self, "_max_samples", 0), 1), max(nr, 1), self.nfields))
+        n = C.c_int()
+        _check(lib().bfam_gpu_domain_get_seismograms(self._h, _dp(out), C.byref(n)))
+        return out[:n.value, :nr].copy()
+
+
+def tile_shapes(dim: int, N: int) -> list[tuple[int, int]]:
+    """(threads per CTA, resident CTAs per SM) of each compiled tile."""
+    L = lib()
+    out = []
+    for t in range(L.bfam_gpu_tile_count(dim, N)):
+        a, b = C.c_int(), C.c_int()
+        _check(L.bfam_gpu_tile_shape(dim, N, t, C.byref(a), C.byref(b)))
+        out.append((a.value, b.value))
+    return out
+
+
+class Batch:
+    """bfam_gpu_batch_t: domains stepped together, one persistent launch per
+    order group and stage."""
+
+    def __init__(self, domains, method: int = LSRK_KC54, t0=None):
+        self.domains = list(domains)
+        hs = (C.c_void_p * len(self.domains))(*[d.handle.value for d in self.domains])
+        t = None if t0 is None else np.ascontiguousarray(
+            np.broadcast_to(t0, (len(self.domains),)), dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().bfam_gpu_batch_create(hs, len(self.domains), method,
+                                           _dp(t) if t is not None else None, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def step(self, dt, nsteps: int = 1, use_graph: bool = True) -> None:
+        dts = np.ascontiguousarray(np.broadcast_to(dt, (len(self.domains),)),
+                                   dtype=np.float64)
+        _check(lib().bfam_gpu_batch_step(self._h, _dp(dts), nsteps, 1 if use_graph else 0))
+
+    def time(self, i: int) -> float:
+        t = C.c_double()
+        _check(lib().bfam_gpu_batch_time(self._h, i, C.byref(t)))
+        return t.value
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().bfam_gpu_batch_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def sync(self) -> None:
+        _check(lib().bfam_gpu_batch_sync(self._h))
+
+    def groups(self) -> list[dict]:
+        L = lib()
+        out = []
+        for g in range(L.bfam_gpu_batch_num_groups(self._h)):
+            d, n, p, k = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+            _check(L.bfam_gpu_batch_group_info(self._h, g, C.byref(d), C.byref(n),
+                                               C.byref(p), C.byref(k)))
+            out.append({"dim": d.value, "N": n.value, "precision": p.value,
+                        "elements": k.value})
+        return out
+
+    def set_tile(self, group: int, tile: int, ctas_per_sm: int = 0) -> None:
+        _check(lib().bfam_gpu_batch_set_tile(self._h, group, tile, ctas_per_sm))
+
+    def free(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().bfam_gpu_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class LSRK:

@@ -16,6 +16,7 @@ import argparse
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent.parent
@@ -33,7 +34,7 @@ def _nvcc() -> str:
 
 
 def _sources() -> list[Path]:
-    return [CSRC / "bfam_gpu.cu"] + sorted((CSRC / "host").glob("*.c"))
+    return sorted(CSRC.glob("*.cu")) + sorted((CSRC / "host").glob("*.c"))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -44,19 +45,31 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 
 def build_product(force: bool = False, verbose: bool = False) -> Path:
-    deps = _sources() + sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h"))
+    headers = (sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h"))
+               + sorted((ROOT / "include").glob("*.h")))
+    deps = _sources() + headers
     if not force and not _stale(LIB, deps):
         return LIB
-    cmd = [
-        _nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17",
-        "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-        "--expt-relaxed-constexpr",
-        "-I", str(ROOT / "include"), "-I", str(CSRC),
-        "-o", str(LIB), *map(str, _sources()),
-    ]
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    flags = [*NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17",
+             "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+             "--expt-relaxed-constexpr",
+             "-I", str(ROOT / "include"), "-I", str(CSRC)]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+        flags.insert(0, "-Xptxas=-v")
+
+    def compile_one(src: Path) -> Path:
+        obj = objdir / (src.name + ".o")
+        if force or _stale(obj, [src] + headers):
+            subprocess.run([_nvcc(), *flags, "-c", "-o", str(obj), str(src)], check=True)
+        return obj
+
+    # translation units compile in parallel (the kernel instantiations dominate)
+    with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, _sources()))
+    subprocess.run([_nvcc(), *NVCC_ARCH, "-shared", "-o", str(LIB), *map(str, objs)],
+                   check=True)
     return LIB
 
 

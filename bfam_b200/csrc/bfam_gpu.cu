@@ -7,6 +7,7 @@
 #include "bfam_gpu.h"
 #include "dg_energy.cuh"
 #include "dg_stage.cuh"
+#include "gpu_internal.h"
 
 #include <atomic>
 #include <cmath>
@@ -18,8 +19,11 @@
 #include <vector>
 
 using namespace bfam_b200;
+using namespace bfam_b200::host;
 
-namespace
+namespace bfam_b200
+{
+namespace host
 {
 
 thread_local std::string g_err;
@@ -36,46 +40,11 @@ int fail(int code, const char *fmt, ...)
   return code;
 }
 
-#define CUDA_TRY(call)                                                         \
-  do                                                                           \
-  {                                                                            \
-    cudaError_t e_ = (call);                                                   \
-    if (e_ != cudaSuccess)                                                     \
-      return fail(BFAM_GPU_ECUDA, "%s: %s (%s:%d)", #call,                     \
-                  cudaGetErrorString(e_), __FILE__, __LINE__);                 \
-  } while (0)
+} // namespace host
+} // namespace bfam_b200
 
-// per-order launchers (the kernels' parameter lists depend on the order)
-typedef void (*stage_launch_fn)(const DomainView &, const StageParams &,
-                                const double *D, int mode, cudaStream_t);
-typedef cudaError_t (*prepare_fn)();
-typedef void (*energy_fn)(const double *, size_t, const ElemData *,
-                          const double *, double *);
-
-struct KernelSet
+namespace
 {
-  stage_launch_fn launch = nullptr;
-  prepare_fn prepare = nullptr;
-  energy_fn energy = nullptr;
-  int NT = 0;
-  size_t smem = 0;
-};
-
-// hops: host copy of the operator block Dr | interp[3] | proj[3] | w
-template <int N, typename CT>
-DiffOp<N, CT> make_diffop(const double *hops)
-{
-  constexpr int n2 = (N + 1) * (N + 1);
-  DiffOp<N, CT> dop;
-  for (int i = 0; i < n2; ++i)
-  {
-    dop.D[i] = CT(hops[i]);
-    dop.Ib[i] = CT(hops[2 * n2 + i]); // interpolation[1]: refine to bottom
-    dop.Pb[i] = hops[5 * n2 + i];     // projection[1]: coarsen from bottom
-  }
-  dop.iwend = 1.0 / hops[7 * n2];
-  return dop;
-}
 
 template <int DIM, int N, typename CT>
 void stage_launch(const DomainView &v, const StageParams &sp,
@@ -123,6 +92,13 @@ template <int DIM, int N, typename CT> KernelSet make_set()
   return k;
 }
 
+} // namespace
+
+namespace bfam_b200
+{
+namespace host
+{
+
 // precision: BFAM_GPU_PRECISION_FP64 (double) or _FP32 (float right-hand side)
 bool kernel_set(int dim, int N, int precision, KernelSet *out)
 {
@@ -140,6 +116,12 @@ bool kernel_set(int dim, int N, int precision, KernelSet *out)
 #undef BFAM_CASE
   return false;
 }
+
+} // namespace host
+} // namespace bfam_b200
+
+namespace
+{
 
 int gmask_host(int dim, int Nq, int f, int pn)
 {
@@ -187,46 +169,9 @@ int face_perm_host(int dim, int Nq, int ns, int pn)
 
 } // namespace
 
-struct bfam_gpu_domain
+namespace bfam_b200
 {
-  int dim = 0, N = 0, Nq = 0, Np = 0, Nfp = 0, NF = 0, NFLD = 0;
-  int32_t K = 0, Kg = 0;
-  int device = 0;
-  int flux = 0, precision = 0;
-  size_t fs = 0;
-  KernelSet ks;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  double *q[2] = {nullptr, nullptr};
-  double *dq = nullptr;
-  double *rhs = nullptr;
-  double *energy = nullptr;
-  ElemData *ed = nullptr;
-  int2 *fdesc = nullptr;
-  int2 *gpart = nullptr;
-  double4 *fcE = nullptr;
-  double4 *fcG = nullptr;
-  double *ops = nullptr;
-  // host copy of Dr | interp[3] | proj[3] | w; the 1-D operators are passed
-  // by value (kernel parameter bank) to each launch
-  std::vector<double> hops;
-  int *err = nullptr;
-  int cur = 0;
-  size_t bytes = 0, budget = 0;
-  std::vector<void *> allocs;
-};
-
-struct bfam_ts_lsrk
-{
-  bfam_gpu_domain_t *dom = nullptr;
-  int ns = 0;
-  double A[6] = {0}, B[6] = {0}, C[7] = {0};
-  double t = 0;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  double graph_dt[2] = {0, 0};
-};
-
-namespace
+namespace host
 {
 
 int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes)
@@ -244,19 +189,24 @@ int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes)
                 cudaGetErrorString(e));
   }
   d->allocs.push_back(*p);
+  d->alloc_bytes.push_back(bytes);
   d->bytes += bytes;
   return 0;
 }
 
-template <typename T>
-int upload(bfam_gpu_domain_t *d, T **dst, const T *src, size_t n)
+void dev_free(bfam_gpu_domain_t *d, void *p)
 {
-  int rc = dev_alloc(d, (void **)dst, n * sizeof(T));
-  if (rc)
-    return rc;
-  if (n)
-    CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
-  return 0;
+  if (!p)
+    return;
+  for (size_t i = 0; i < d->allocs.size(); ++i)
+    if (d->allocs[i] == p)
+    {
+      cudaFree(p);
+      d->bytes -= d->alloc_bytes[i];
+      d->allocs.erase(d->allocs.begin() + i);
+      d->alloc_bytes.erase(d->alloc_bytes.begin() + i);
+      return;
+    }
 }
 
 void release(bfam_gpu_domain_t *d)
@@ -288,16 +238,20 @@ DomainView view(bfam_gpu_domain_t *d, int in)
   v.fcG = d->fcG;
   v.ops = d->ops;
   v.err = d->err;
+  v.dt = 0;
+  v.src = d->src;
+  v.clock = d->clock;
   return v;
 }
 
-int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double dt,
-                 int first, int mode)
+int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double C,
+                 double dt, int first, int mode)
 {
   StageParams sp;
   sp.A = A;
   sp.B = B;
   sp.dt = dt;
+  sp.C = C;
   sp.first_stage = first;
   sp.flux = d->flux;
   DomainView v = view(d, in);
@@ -308,7 +262,8 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double dt,
   return 0;
 }
 
-} // namespace
+} // namespace host
+} // namespace bfam_b200
 
 extern "C" {
 
@@ -653,11 +608,18 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
   TRY(upload(d, &d->fcG, fcG.data(), fcG.size()));
   TRY(upload(d, &d->ops, ops.data(), ops.size()));
   TRY(dev_alloc(d, (void **)&d->err, sizeof(int)));
+  TRY(dev_alloc(d, (void **)&d->clock, sizeof(DomainClock)));
 #undef TRY
+  // host copies for locating sources and receivers
+  d->hx0.assign(vol->x0, vol->x0 + 3 * (size_t)vol->K);
+  d->hh.assign(vol->h, vol->h + 3 * (size_t)vol->K);
+  d->hr.assign(vol->r, vol->r + d->Nq);
+  d->hw.assign(vol->w, vol->w + d->Nq);
   if (cudaMemset(d->q[0], 0, state) != cudaSuccess ||
       cudaMemset(d->q[1], 0, state) != cudaSuccess ||
       cudaMemset(d->dq, 0, state) != cudaSuccess ||
-      cudaMemset(d->err, 0, sizeof(int)) != cudaSuccess)
+      cudaMemset(d->err, 0, sizeof(int)) != cudaSuccess ||
+      cudaMemset(d->clock, 0, sizeof(DomainClock)) != cudaSuccess)
   {
     release(d);
     return fail(BFAM_GPU_ECUDA, "initial memset failed");
@@ -772,7 +734,7 @@ int bfam_gpu_domain_rhs(bfam_gpu_domain_t *d, double *const *rhs)
     if (rc)
       return rc;
   }
-  int rc = launch_stage(d, d->cur, 0.0, 0.0, 0.0, 1, MODE_RHS);
+  int rc = launch_stage(d, d->cur, 0.0, 0.0, 0.0, 0.0, 1, MODE_RHS);
   if (rc)
     return rc;
   for (int f = 0; f < d->NFLD; ++f)
@@ -873,6 +835,7 @@ int bfam_ts_lsrk_init(bfam_ts_lsrk_t **ts, bfam_gpu_domain_t *dom, int method,
   bfam_ts_lsrk_t *s = new bfam_ts_lsrk_t();
   s->dom = dom;
   s->t = t0;
+  dom->clock_valid = false; // set from t0 before the first step that needs it
   switch (method)
   {
   case 0: // KC54: Carpenter & Kennedy five-stage fourth-order
@@ -932,12 +895,35 @@ int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
     return fail(BFAM_GPU_EINVAL, "bad arguments");
   bfam_gpu_domain_t *d = ts->dom;
   CUDA_TRY(cudaSetDevice(d->device));
+  // a point source or receivers need the device clock, advanced once per
+  // step by the post-step kernel
+  const bool post = has_extras(d);
+  if (post && !d->clock_valid)
+  {
+    int rc = set_clock(d, ts->t, 0);
+    if (rc)
+      return rc;
+  }
+  // one step starting from state buffer c0
+  auto issue = [&](int c0) -> int {
+    int in = c0;
+    for (int s = 0; s < ts->ns; ++s, in ^= 1)
+    {
+      int rc = launch_stage(d, in, ts->A[s], ts->B[s], ts->C[s], dt, s == 0,
+                            MODE_STAGE);
+      if (rc)
+        return rc;
+    }
+    return post ? launch_post(d, in, dt) : 0;
+  };
+  const int per_step = ts->ns + (post ? 1 : 0);
   for (int st = 0; st < nsteps; ++st)
   {
     const int c0 = d->cur;
     if (use_graph && d->stream)
     {
-      if (!ts->graph[c0] || ts->graph_dt[c0] != dt)
+      if (!ts->graph[c0] || ts->graph_dt[c0] != dt ||
+          ts->graph_post[c0] != post || ts->graph_gen[c0] != d->extras_gen)
       {
         if (ts->graph[c0])
           cudaGraphExecDestroy(ts->graph[c0]);
@@ -945,9 +931,7 @@ int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
         cudaGraph_t g;
         CUDA_TRY(cudaStreamBeginCapture(d->stream,
                                         cudaStreamCaptureModeThreadLocal));
-        int in = c0, rc = 0;
-        for (int s = 0; s < ts->ns && !rc; ++s, in ^= 1)
-          rc = launch_stage(d, in, ts->A[s], ts->B[s], dt, s == 0, MODE_STAGE);
+        const int rc = issue(c0);
         cudaError_t ce = cudaStreamEndCapture(d->stream, &g);
         if (rc)
           return rc;
@@ -960,26 +944,25 @@ int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
           return fail(BFAM_GPU_ECUDA, "graph instantiate: %s",
                       cudaGetErrorString(ce));
         ts->graph_dt[c0] = dt;
+        ts->graph_post[c0] = post;
+        ts->graph_gen[c0] = d->extras_gen;
         // capture counted the launches once; replays are counted below
-        g_launches.fetch_sub(ts->ns, std::memory_order_relaxed);
+        g_launches.fetch_sub(per_step, std::memory_order_relaxed);
       }
       CUDA_TRY(cudaGraphLaunch(ts->graph[c0], d->stream));
-      g_launches.fetch_add(ts->ns, std::memory_order_relaxed);
+      g_launches.fetch_add(per_step, std::memory_order_relaxed);
     }
     else
     {
-      int in = c0;
-      for (int s = 0; s < ts->ns; ++s, in ^= 1)
-      {
-        int rc = launch_stage(d, in, ts->A[s], ts->B[s], dt, s == 0,
-                              MODE_STAGE);
-        if (rc)
-          return rc;
-      }
+      const int rc = issue(c0);
+      if (rc)
+        return rc;
     }
     d->cur = (ts->ns & 1) ? c0 ^ 1 : c0;
     ts->t += dt;
   }
+  if (!post && nsteps > 0)
+    d->clock_valid = false;
   return 0;
 }
 

@@ -26,6 +26,26 @@ struct ElemData
 // Glue partner, one per glue element g (used on the coarse side):
 //   a = partner (fine) element, b & 7 = partner face, b>>3 & 7 = orientation,
 //   b>>6 & 7 = hanging piece of g.
+// Per-domain clock in device memory, advanced once per time step by the
+// post-step kernel, so that replayed CUDA graphs see the current time.
+struct DomainClock
+{
+  double time; // time at the start of the current step
+  int nsamp;   // receiver samples recorded
+  int pad;
+};
+
+// Ricker point force of a domain (src_elem < 0: none).  Per node of the
+// source element, src_w = phi_n(x_s) / (w_n J): the point force projected on
+// the Lagrange basis through the lumped LGL mass.
+struct PointSource
+{
+  int elem;
+  const double *__restrict__ w; // [Np]
+  double force[3];              // force vector (amplitude and direction)
+  double f0, t0;                // peak frequency, time of the peak
+};
+
 struct DomainView
 {
   int32_t K;
@@ -43,14 +63,26 @@ struct DomainView
   const double *__restrict__ ops;  // Dr | interp[3] | proj[3] | w
   int *err;
   double dt; // time step of this domain (batches step domains with their own)
+  PointSource src;
+  const DomainClock *clock;
 };
 
 struct StageParams
 {
   double A, B, dt;
+  double C;        // stage time t + C dt
   int first_stage; // A == 0: dq is not read
   int flux;        // 0 upwind, 1 central
 };
+
+// Ricker wavelet (1 - 2 a) exp(-a), a = (pi f0 (t - t0))^2
+__host__ __device__ inline double ricker(double t, double f0, double t0)
+{
+  const double pi = 3.14159265358979323846;
+  const double x = pi * f0 * (t - t0);
+  const double a = x * x;
+  return (1.0 - 2.0 * a) * exp(-a);
+}
 
 // The 1-D operators travel in the kernel's parameter space so that their
 // entries, indexed by unrolled loop counters, are constant-bank operands of

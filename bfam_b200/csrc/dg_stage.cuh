@@ -489,6 +489,16 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
         acc[c] += lc[c * Nfp];
     }
 
+    // point source on the velocity: s f(t_stage) F phi_n(x_s) / (rho w_n J)
+    if (e == d.src.elem)
+    {
+      const double ts = d.clock->time + sp.C * d.dt;
+      const double g = s * ricker(ts, d.src.f0, d.src.t0) * d.src.w[n] * me.irho;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+        acc[c] += g * d.src.force[c];
+    }
+
     if constexpr (MODE == MODE_STAGE)
     {
       if (rd)
@@ -565,8 +575,7 @@ __global__ void __launch_bounds__(NT, MINB)
   for (int i = blockIdx.x; i < nwork; i += gridDim.x, ++iter)
   {
     const int2 w = work[i];
-    const DomainView d = views[w.x];
-    stage_element<DIM, N, NT, MODE, CT>(d, sp, dop, w.y, iter);
+    stage_element<DIM, N, NT, MODE, CT>(views[w.x], sp, dop, w.y, iter);
     __syncthreads(); // shared memory is reused by the next element
   }
 }

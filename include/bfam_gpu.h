@@ -190,6 +190,87 @@ int bfam_ts_lsrk_free(bfam_ts_lsrk_t *ts);
 /* Wait for the domain's stream and report device-side errors. */
 int bfam_gpu_domain_sync(bfam_gpu_domain_t *dom);
 
+/* ------------------------------------------------------------------------
+ * Point source and receivers (the serving requests' solves).  No
+ * counterpart in the reference: bfam's DG path has no sources or receivers
+ * (its applications supplied their own).  With either present, every LSRK
+ * step ends with one post-step launch that samples the receivers and
+ * advances the domain's device clock (the source's time base).
+ * ---------------------------------------------------------------------- */
+
+/* Ricker-wavelet point force f(t) F, f(t) = (1 - 2a) exp(-a),
+ * a = (pi f0 (t - t0))^2, added to the velocity equation as
+ * f(t) F phi_n(x) / (rho w_n J) at the nodes n of the element holding x
+ * (the point force projected on the Lagrange basis with the lumped LGL
+ * mass).  The element holding x is the one whose half-open box
+ * [x0, x0 + h) contains it. */
+typedef struct
+{
+  double x[3];     /* location (z ignored in 2D) */
+  double force[3]; /* force vector F */
+  double f0;       /* peak frequency */
+  double t0;       /* time of the peak */
+} bfam_gpu_source_t;
+
+/* Set (src != NULL) or remove (NULL) the domain's point source.
+ * BFAM_GPU_EINVAL if x lies in no element. */
+int bfam_gpu_domain_set_source(bfam_gpu_domain_t *dom,
+                               const bfam_gpu_source_t *src);
+
+/* Receivers at nrecv points x[r*3 + a]: after every step each field is
+ * interpolated (Lagrange basis of the element holding the point) and stored
+ * as sample s of receiver r.  Keeps at most max_samples samples; resets
+ * the sample count.  nrecv == 0 removes the receivers. */
+int bfam_gpu_domain_set_receivers(bfam_gpu_domain_t *dom, int nrecv,
+                                  const double *x, int max_samples);
+
+/* Copy the recorded samples, out[(s*nrecv + r)*num_fields + f], and their
+ * count (at most max_samples) into *nsamples.  Synchronises the domain's
+ * stream. */
+int bfam_gpu_domain_get_seismograms(bfam_gpu_domain_t *dom, double *out,
+                                    int *nsamples);
+
+/* ------------------------------------------------------------------------
+ * Batches: many independent domains stepped together.  No counterpart in
+ * the reference (one bfam domain per MPI rank).  Domains are grouped by
+ * (dim, order, precision, flux, operators); each group is one persistent
+ * launch per LSRK stage over a flat (domain, element) work list, the groups
+ * run on forked streams, and a step is replayed from a CUDA graph.  The
+ * domains keep their own state, time step and clock; a domain must not be
+ * stepped by another stepper while it belongs to a batch.
+ * ---------------------------------------------------------------------- */
+typedef struct bfam_gpu_batch bfam_gpu_batch_t;
+
+/* ndom domains on one device; t0[i] is domain i's start time (NULL: 0). */
+int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
+                          int method, const double *t0,
+                          bfam_gpu_batch_t **out);
+/* Launch on this stream (NULL: the batch's own stream). */
+int bfam_gpu_batch_set_stream(bfam_gpu_batch_t *b, void *stream);
+/* Advance every domain nsteps steps, domain i with step dt[i]. */
+int bfam_gpu_batch_step(bfam_gpu_batch_t *b, const double *dt, int nsteps,
+                        int use_graph);
+int bfam_gpu_batch_time(const bfam_gpu_batch_t *b, int i, double *t);
+/* Wait for the batch's stream and report device-side errors. */
+int bfam_gpu_batch_sync(bfam_gpu_batch_t *b);
+int bfam_gpu_batch_free(bfam_gpu_batch_t *b);
+/* Number of order groups, and group g's (dim, N, precision, elements). */
+int bfam_gpu_batch_num_groups(const bfam_gpu_batch_t *b);
+int bfam_gpu_batch_group_info(const bfam_gpu_batch_t *b, int g, int *dim,
+                              int *N, int *precision, int64_t *elements);
+
+/* Tile shapes compiled for an order: tile t has `threads` threads per CTA
+ * (one element per CTA, one thread per node and per face node; a tile with
+ * fewer threads than nodes loops over the nodes) and a register budget for
+ * `min_ctas` resident CTAs per SM.  Tile 0 is the single-domain kernel's. */
+int bfam_gpu_tile_count(int dim, int N);
+int bfam_gpu_tile_shape(int dim, int N, int tile, int *threads,
+                        int *min_ctas);
+/* Choose group g's tile and persistent grid (ctas_per_sm CTAs per SM; 0:
+ * as many as fit). */
+int bfam_gpu_batch_set_tile(bfam_gpu_batch_t *b, int g, int tile,
+                            int ctas_per_sm);
+
 /* Kernel launches issued by this library since process start. */
 uint64_t bfam_gpu_launch_count(void);
 

@@ -244,6 +244,11 @@ typedef struct
   int32_t *owner; /* finest cell -> element */
   int flux;       /* 0 upwind, 1 central */
   double *work;   /* lsrk dq + rhs */
+  /* Ricker point force (src_elem < 0: none): per node of the source element
+   * phi_n(x_s) / (w_n J) */
+  int32_t src_elem;
+  double *src_W;
+  double src_force[3], src_f0, src_t0;
 } oracle_t;
 
 static int32_t owner_at(const oracle_t *o, int x, int y, int z)
@@ -270,6 +275,7 @@ oracle_t *oracle_new(int dim, int N, int32_t K, const int32_t *ecoord,
   o->NFLD = dim == 3 ? 9 : 5;
   o->K = K;
   o->flux = flux;
+  o->src_elem = -1;
   o->ec = ecoord;
   for (int a = 0; a < 3; ++a)
   {
@@ -321,7 +327,111 @@ void oracle_free(oracle_t *o)
   free(o->lam);
   free(o->mu);
   free(o->work);
+  free(o->src_W);
   free(o);
+}
+
+/* Element holding x: the owner of the finest cell floor(x / unit) (cells
+ * are half-open), and x's reference coordinates in it.  -1 if x is outside
+ * the brick. */
+static int32_t locate(const oracle_t *o, const double *x, double *xi)
+{
+  int c[3] = {0, 0, 0};
+  for (int a = 0; a < o->dim; ++a)
+  {
+    const double f = floor(x[a] / o->unit[a]);
+    if (!(f >= 0 && f < o->D[a]))
+      return -1;
+    c[a] = (int)f;
+  }
+  const int32_t e = owner_at(o, c[0], c[1], c[2]);
+  const int32_t *ce = o->ec + 4 * e;
+  for (int a = 0; a < 3; ++a)
+    xi[a] = a < o->dim
+                ? 2.0 * (x[a] - ce[a] * o->unit[a]) / (ce[3] * o->unit[a]) - 1.0
+                : 0.0;
+  return e;
+}
+
+/* phi_n(x) of the element's nodes (barycentric Lagrange basis) */
+static void node_basis(const oracle_t *o, const double *xi, double *phi)
+{
+  double lam[MAXQ], L[3][MAXQ];
+  bary_weights(o->Nq, o->r, lam);
+  for (int a = 0; a < 3; ++a)
+  {
+    if (a < o->dim)
+      lagrange_eval(o->Nq, o->r, lam, xi[a], L[a]);
+    else
+      for (int i = 0; i < o->Nq; ++i)
+        L[a][i] = 1.0;
+  }
+  for (int n = 0; n < o->Np; ++n)
+  {
+    const int i = n % o->Nq, j = (n / o->Nq) % o->Nq, k = n / (o->Nq * o->Nq);
+    phi[n] = L[0][i] * L[1][j] * (o->dim == 3 ? L[2][k] : 1.0);
+  }
+}
+
+/* Ricker point force f(t) F at x, f(t) = (1 - 2a) exp(-a),
+ * a = (pi f0 (t - t0))^2, on the velocity equation: the point force
+ * projected on the Lagrange basis through the lumped LGL mass.  Returns -1
+ * if x is outside the brick. */
+int oracle_set_source(oracle_t *o, const double *x, const double *force,
+                      double f0, double t0)
+{
+  double xi[3];
+  const int32_t e = locate(o, x, xi);
+  if (e < 0)
+    return -1;
+  if (!o->src_W)
+    o->src_W = malloc(sizeof(double) * o->Np);
+  node_basis(o, xi, o->src_W);
+  const int32_t *ce = o->ec + 4 * e;
+  double J = 1;
+  for (int a = 0; a < o->dim; ++a)
+    J *= 0.5 * ce[3] * o->unit[a];
+  for (int n = 0; n < o->Np; ++n)
+  {
+    const int i = n % o->Nq, j = (n / o->Nq) % o->Nq, k = n / (o->Nq * o->Nq);
+    const double wn = o->w[i] * o->w[j] * (o->dim == 3 ? o->w[k] : 1.0);
+    o->src_W[n] /= wn * J;
+  }
+  o->src_elem = e;
+  for (int a = 0; a < 3; ++a)
+    o->src_force[a] = a < o->dim ? force[a] : 0.0;
+  o->src_f0 = f0;
+  o->src_t0 = t0;
+  return 0;
+}
+
+/* every field interpolated at nrecv points x[3r..]: out[r * NFLD + c].
+ * Returns -1 if a point is outside the brick. */
+int oracle_sample(const oracle_t *o, const double *q, int nrecv,
+                  const double *x, double *out)
+{
+  const size_t fs = (size_t)o->K * o->Np;
+  double *phi = malloc(sizeof(double) * o->Np);
+  for (int r = 0; r < nrecv; ++r)
+  {
+    double xi[3];
+    const int32_t e = locate(o, x + 3 * r, xi);
+    if (e < 0)
+    {
+      free(phi);
+      return -1;
+    }
+    node_basis(o, xi, phi);
+    for (int c = 0; c < o->NFLD; ++c)
+    {
+      double s = 0;
+      for (int n = 0; n < o->Np; ++n)
+        s += phi[n] * q[c * fs + (size_t)e * o->Np + n];
+      out[r * o->NFLD + c] = s;
+    }
+  }
+  free(phi);
+  return 0;
 }
 
 /* volume node of face node q on face f */
@@ -729,9 +839,17 @@ static int lsrk_table(int method, double *A, double *B, double *C)
   return -1;
 }
 
-/* nsteps of 2N-storage LSRK (KC54) on q, in place */
-int oracle_lsrk(oracle_t *o, double *q, double dt, int nsteps, int method,
-                int nthreads)
+static double ricker(double t, double f0, double t0)
+{
+  const double pi = 3.14159265358979323846;
+  const double x = pi * f0 * (t - t0);
+  return (1.0 - 2.0 * x * x) * exp(-x * x);
+}
+
+/* nsteps of 2N-storage LSRK (KC54) on q, in place, from time t; the point
+ * source (if set) is evaluated at the stage times t + C_s dt */
+int oracle_lsrk_from(oracle_t *o, double *q, double t, double dt, int nsteps,
+                     int method, int nthreads)
 {
   double A[6], B[6], C[7];
   const int ns = lsrk_table(method, A, B, C);
@@ -743,10 +861,19 @@ int oracle_lsrk(oracle_t *o, double *q, double dt, int nsteps, int method,
   double *dq = o->work, *rhs = o->work + n;
   memset(dq, 0, sizeof(double) * n);
   set_threads(nthreads);
-  for (int st = 0; st < nsteps; ++st)
+  for (int st = 0; st < nsteps; ++st, t += dt)
     for (int s = 0; s < ns; ++s)
     {
       oracle_rhs(o, q, rhs, nthreads);
+      if (o->src_elem >= 0)
+      {
+        const double f = ricker(t + C[s] * dt, o->src_f0, o->src_t0);
+        const int32_t e = o->src_elem;
+        for (int a = 0; a < o->dim; ++a)
+          for (int n = 0; n < o->Np; ++n)
+            rhs[a * (size_t)o->K * o->Np + (size_t)e * o->Np + n] +=
+                f * o->src_force[a] * o->src_W[n] / o->rho[e];
+      }
 #pragma omp parallel for schedule(static)
       for (size_t i = 0; i < n; ++i)
       {
@@ -805,4 +932,10 @@ double oracle_energy(const oracle_t *o, const double *q)
     E += 0.5 * J * Ee;
   }
   return E;
+}
+
+int oracle_lsrk(oracle_t *o, double *q, double dt, int nsteps, int method,
+                int nthreads)
+{
+  return oracle_lsrk_from(o, q, 0.0, dt, nsteps, method, nthreads);
 }

@@ -35,6 +35,10 @@ def lib() -> C.CDLL:
         L.oracle_free.argtypes = [C.c_void_p]
         L.oracle_rhs.argtypes = [C.c_void_p, dp, dp, C.c_int]
         L.oracle_lsrk.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.oracle_lsrk_from.argtypes = [C.c_void_p, dp, C.c_double, C.c_double, C.c_int,
+                                       C.c_int, C.c_int]
+        L.oracle_set_source.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_double]
+        L.oracle_sample.argtypes = [C.c_void_p, dp, C.c_int, dp, dp]
         L.oracle_energy.restype = C.c_double
         L.oracle_energy.argtypes = [C.c_void_p, dp]
         L.oracle_lgl_nodes.argtypes = [C.c_int, dp, dp]
@@ -111,6 +115,43 @@ class Oracle:
         if rc:
             raise ValueError("unsupported LSRK method for the oracle")
         return q
+
+    def lsrk_from(self, q: np.ndarray, t: float, dt: float, nsteps: int,
+                  nthreads: int = 0, method: int = 0) -> np.ndarray:
+        """nsteps from time t (the point source is time dependent)"""
+        q = np.array(q, dtype=np.float64, order="C", copy=True)
+        rc = lib().oracle_lsrk_from(self._h, _dp(q), t, dt, nsteps, method, nthreads)
+        if rc:
+            raise ValueError("unsupported LSRK method for the oracle")
+        return q
+
+    def set_source(self, x, force, f0: float, t0: float) -> None:
+        xv = np.zeros(3)
+        fv = np.zeros(3)
+        xv[:len(x)] = x
+        fv[:len(force)] = force
+        if lib().oracle_set_source(self._h, _dp(xv), _dp(fv), f0, t0):
+            raise ValueError("source point outside the brick")
+
+    def sample(self, q: np.ndarray, x: np.ndarray) -> np.ndarray:
+        """fields at points x [nrecv][3] -> [nrecv][nfields]"""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, 3))
+        out = np.empty((len(x), q.shape[0]))
+        if lib().oracle_sample(self._h, _dp(q), len(x), _dp(x), _dp(out)):
+            raise ValueError("receiver outside the brick")
+        return out
+
+    def seismograms(self, q: np.ndarray, t: float, dt: float, nsteps: int,
+                    x: np.ndarray, nthreads: int = 0):
+        """step nsteps from time t, sampling x after every step: returns the
+        final state and samples [nsteps][nrecv][nfields]"""
+        out = []
+        for _ in range(nsteps):
+            q = self.lsrk_from(q, t, dt, 1, nthreads)
+            t += dt
+            out.append(self.sample(q, x))
+        return q, np.array(out)
 
     def energy(self, q: np.ndarray) -> float:
         q = np.ascontiguousarray(q, dtype=np.float64)

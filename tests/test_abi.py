@@ -120,3 +120,34 @@ def test_rejects_bad_material_and_order():
     v2 = _vol(bf.Mesh(3, 9, (1, 1, 1)), keep)
     rc, _ = _create(v2)
     assert rc == -5
+
+
+def test_batch_and_extras_reject_bad_arguments_without_a_device():
+    L = bf.lib()
+    h = C.c_void_p()
+    assert L.bfam_gpu_batch_create(None, 0, 0, None, C.byref(h)) == bf.BFAM_GPU_EINVAL
+    assert L.bfam_gpu_batch_create(None, 1, 0, None, None) == bf.BFAM_GPU_EINVAL
+    assert L.bfam_gpu_batch_step(None, None, 1, 1) == bf.BFAM_GPU_EINVAL
+    assert L.bfam_gpu_batch_set_tile(None, 0, 0, 0) == bf.BFAM_GPU_EINVAL
+    assert L.bfam_gpu_batch_num_groups(None) == 0
+    assert L.bfam_gpu_batch_free(None) == 0
+    assert L.bfam_gpu_domain_set_source(None, None) == bf.BFAM_GPU_EINVAL
+    assert L.bfam_gpu_domain_set_receivers(None, 1, None, 1) == bf.BFAM_GPU_EINVAL
+    n = C.c_int()
+    assert L.bfam_gpu_domain_get_seismograms(None, None, C.byref(n)) == bf.BFAM_GPU_EINVAL
+
+
+def test_tile_table():
+    # tile 0 is the single-domain kernel's shape; every tile has one thread
+    # per face node at least
+    for dim, orders in ((2, range(1, 9)), (3, range(1, 8))):
+        for N in orders:
+            shapes = bf.tile_shapes(dim, N)
+            assert shapes, (dim, N)
+            nfp = (N + 1) ** (dim - 1)
+            for threads, minb in shapes:
+                assert threads % 32 == 0 and threads >= 2 * dim * nfp and minb >= 1
+    assert len(bf.tile_shapes(3, 5)) == 3 and len(bf.tile_shapes(3, 7)) == 2
+    assert bf.lib().bfam_gpu_tile_count(3, 9) == 0
+    a, b = C.c_int(), C.c_int()
+    assert bf.lib().bfam_gpu_tile_shape(3, 5, 7, C.byref(a), C.byref(b)) == bf.BFAM_GPU_EINVAL
