@@ -13,6 +13,10 @@ elements visited in Morton order).
   cfg2  cfg1's mesh and material at N=7 (heterogeneous, for throughput and
         error against the FP64 path); homogeneous variant with the plane wave
         k=(2pi,0,0) for the analytic error over one period
+  cfg3  256 independent 3D instances: final element count K drawn
+        log-uniform in [512, 32768] (seed 1), order from {3, 5, 7}, base
+        brick of about K / 2.4 cells refined once with p = 0.2, cfg1's
+        material law and a Gaussian pulse; precision form
 Time step: dt = CFL * min_e(min_a h_{e,a} / cp_e) / N^2.
 """
 from __future__ import annotations
@@ -22,7 +26,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Mesh, lgl_operators, material_random
+from . import PCG32, Mesh, lgl_operators, material_random
 
 
 @dataclass
@@ -62,8 +66,8 @@ def cfg0() -> Problem:
 
 def heterogeneous_brick(N: int, n: int = 32, refine_prob: float = 0.3, seed: int = 0,
                         width: float = 0.05, nsteps: int = 200, cfl: float = 0.5,
-                        name: str = "cfg1") -> Problem:
-    mesh = Mesh(3, N, (n, n, n), refine_prob=refine_prob, seed=seed)
+                        name: str = "cfg1", dims=None) -> Problem:
+    mesh = Mesh(3, N, dims or (n, n, n), refine_prob=refine_prob, seed=seed)
     r = lgl_operators(N)[0]
     rho, lam, mu = material_random(mesh.K, seed)
     q0 = mesh.gaussian_pulse(r, (0.5, 0.5, 0.5), width)
@@ -94,3 +98,32 @@ def plane_wave_3d(N: int, n: int, refine_prob: float = 0.3, seed: int = 0,
     nsteps = int(math.ceil(T / dt0))
     return Problem(f"plane_wave_N{N}_n{n}", mesh, rho, lam, mu, q0, T / nsteps, nsteps,
                    {"k": k, "T": T})
+
+
+def cfg3_specs(count: int = 256, seed: int = 1, orders=(3, 5, 7), kmin: int = 512,
+               kmax: int = 32768, refine_prob: float = 0.2) -> list[dict]:
+    """Instance draws of the batching workload (PCG32 seed `seed`, stream 3):
+    K log-uniform in [kmin, kmax] is the target final element count; the
+    base brick has about K / (1 + 7 p) cells, as close to a cube as whole
+    cells allow."""
+    g = PCG32(seed, 3)
+    out = []
+    for i in range(count):
+        u = g.uniform()
+        K = math.exp(math.log(kmin) + u * (math.log(kmax) - math.log(kmin)))
+        N = orders[g.bounded(len(orders))]
+        base = K / (1 + 7 * refine_prob)
+        nx = max(1, round(base ** (1.0 / 3.0)))
+        nz = max(1, round(base / (nx * nx)))
+        out.append({"index": i, "N": N, "n": (nx, nx, nz), "K_target": K,
+                    "refine_prob": refine_prob, "seed": seed * 100000 + i})
+    return out
+
+
+def cfg3_instance(spec: dict, width: float = 0.05, cfl: float = 0.5,
+                  nsteps: int = 100) -> Problem:
+    p = heterogeneous_brick(spec["N"], n=1, refine_prob=spec["refine_prob"],
+                            seed=spec["seed"], width=width, nsteps=nsteps, cfl=cfl,
+                            name=f"cfg3[{spec['index']}]", dims=spec["n"])
+    p.meta.update(spec)
+    return p
