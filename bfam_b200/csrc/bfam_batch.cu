@@ -595,8 +595,6 @@ int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
   b->gen.assign(ndom, 0);
   b->dt.assign(ndom, 0.0);
   b->t.assign(ndom, 0.0);
-  for (int i = 0; i < ndom; ++i)
-    b->t[i] = t0 ? t0[i] : 0.0;
 #define TRY(x)                                                                 \
   do                                                                           \
   {                                                                            \
@@ -681,15 +679,29 @@ int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
   }
   for (int p = 0; p < 2; ++p)
     TRY(batch_alloc(b, (void **)&b->post[p], ndom * sizeof(PostView)));
-  // device clocks from the start times
+  // device clocks: set from t0, or kept (read back) without it
   for (int i = 0; i < ndom; ++i)
   {
-    dg_set_clock_kernel<<<1, 1, 0, b->stream>>>(doms[i]->clock, b->t[i], 1);
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (t0)
+    {
+      b->t[i] = t0[i];
+      dg_set_clock_kernel<<<1, 1, 0, doms[i]->stream>>>(doms[i]->clock, t0[i],
+                                                         1);
+      g_launches.fetch_add(1, std::memory_order_relaxed);
+      CTRY(cudaGetLastError());
+    }
+    else
+    {
+      DomainClock c;
+      CTRY(cudaMemcpyAsync(&c, doms[i]->clock, sizeof(c),
+                           cudaMemcpyDeviceToHost, doms[i]->stream));
+      CTRY(cudaStreamSynchronize(doms[i]->stream));
+      b->t[i] = c.time;
+    }
     doms[i]->clock_valid = true;
   }
-  CTRY(cudaGetLastError());
-  CTRY(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < ndom; ++i)
+    CTRY(cudaStreamSynchronize(doms[i]->stream));
 #undef CTRY
 #undef TRY
   *out = b;

@@ -241,7 +241,9 @@ int bfam_gpu_domain_get_seismograms(bfam_gpu_domain_t *dom, double *out,
  * ---------------------------------------------------------------------- */
 typedef struct bfam_gpu_batch bfam_gpu_batch_t;
 
-/* ndom domains on one device; t0[i] is domain i's start time (NULL: 0). */
+/* ndom domains on one device; t0[i] is domain i's start time (NULL: each
+ * domain keeps the time of its device clock, which starts at 0 and is
+ * advanced by every step that has a post-step launch). */
 int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
                           int method, const double *t0,
                           bfam_gpu_batch_t **out);
