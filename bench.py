@@ -44,7 +44,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--config", default="cfg1",
+                    choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--rates", default="10,50,200,500",
+                    help="cfg4: Poisson arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate")
+    ap.add_argument("--chunk", type=int, default=25, help="cfg4: steps per batch chunk")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="arithmetic of the right-hand side (default: fp64; cfg3: fp32)")
     ap.add_argument("--instances", type=int, default=256, help="cfg3: number of instances")
@@ -388,12 +393,93 @@ def run_batched(args):
     return 0
 
 
+def run_serving(args):
+    """cfg4: Poisson streams of point-source requests through the
+    continuous-batching server, one run per arrival rate."""
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    import bfam_b200 as bf
+    from bfam_b200 import autotune, serving
+    from oracle import oracle as orc
+
+    prec = bf.PRECISION_FP64 if args.precision == "fp64" else bf.PRECISION_FP32
+    # tile choices for the request orders, before any clock starts
+    for N in (3, 5):
+        m = bf.Mesh(3, N, (8, 8, 8))
+        d = bf.GpuDomain(m, 1.0, 2.0, 1.0, precision=prec, device=local)
+        b = bf.Batch([d])
+        autotune.autotune(b, device=local)
+        b.free()
+        d.free()
+    runs = []
+    checks = []
+    n0 = bf.launch_count()
+    with ClockSampler(local) as clk:
+        for rate in [float(x) for x in args.rates.split(",")]:
+            reqs = serving.poisson_requests(rate, args.requests, seed=2)
+            srv = serving.Server(serving.GpuEngine(prec, device=local),
+                                 budget_bytes=150 * 10 ** 9, chunk=args.chunk)
+            stats = srv.run(reqs, realtime=True)
+            s = stats.summary()
+            s["rate_per_s"] = rate
+            s["requests"] = len(reqs)
+            runs.append(s)
+            # accuracy: the smallest requests against the FP64 oracle; one
+            # request re-solved alone on the GPU must match bitwise
+            for r in sorted(reqs, key=lambda r: r.n ** 3 * (r.N + 1) ** 3 * r.nsteps)[:2]:
+                mesh, rho, lam, mu, dt = serving.request_problem(r)
+                o = orc.Oracle.from_mesh(mesh, rho, lam, mu)
+                o.set_source(r.source, r.force, r.f0, r.t0)
+                _, ref = o.seismograms(mesh.empty_fields(), 0.0, dt, r.nsteps, r.receivers,
+                                       nthreads=orc.max_threads())
+                e = float(np.sqrt(((r.seismograms - ref) ** 2).sum() / (ref ** 2).sum()))
+                checks.append({"rate": rate, "request": r.id, "n": r.n, "N": r.N,
+                               "steps": r.nsteps, "rel_l2_vs_fp64_oracle": e})
+            r = reqs[len(reqs) // 2]
+            mesh, rho, lam, mu, dt = serving.request_problem(r)
+            d = bf.GpuDomain(mesh, rho, lam, mu, precision=prec, device=local)
+            d.set_source(r.source, r.force, r.f0, r.t0)
+            d.set_receivers(r.receivers, r.nsteps)
+            bf.LSRK(d).step(dt, r.nsteps, use_graph=True)
+            checks.append({"rate": rate, "request": r.id,
+                           "alone_equals_in_mix": bool(np.array_equal(d.seismograms(),
+                                                                      r.seismograms))})
+            d.free()
+    launches = bf.launch_count() - n0
+    worst = max(c.get("rel_l2_vs_fp64_oracle", 0.0) for c in checks)
+    if rank == 0:
+        top = max(runs, key=lambda s: s["dof_updates_per_s"])
+        line = {
+            "metric": "DOF-updates/s (serving; p50/p99 latency per rate)",
+            "value": top["dof_updates_per_s"], "unit": "DOF-updates/s",
+            "n_gpus": ws, "steps": sum(s["chunks"] for s in runs), "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 rhs / f64 state" if prec == bf.PRECISION_FP32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": "cfg4: Poisson request streams (seed 2), bricks 8^3-24^3, "
+                                   "N in {3,5}, 50-400 LSRK steps, Ricker point force, "
+                                   "16 receivers, 150 GB budget, continuous batching",
+                       "requests_per_rate": args.requests, "chunk_steps": args.chunk,
+                       "parallelism": f"replicas{ws}"},
+            "serving": runs, "accuracy": {"max_rel_l2_vs_fp64_oracle": worst,
+                                          "checks": checks},
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "cfg3":
         return run_batched(args)
+    if args.config == "cfg4":
+        return run_serving(args)
     import torch
     ws, rank, local = dist_init()
     torch.cuda.set_device(local)
