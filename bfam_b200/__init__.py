@@ -138,6 +138,8 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_batch_time": (C.c_int, [vp, C.c_int, dp]),
         "bfam_gpu_batch_sync": (C.c_int, [vp]),
         "bfam_gpu_batch_free": (C.c_int, [vp]),
+        "bfam_gpu_batch_launches_per_step": (C.c_int, [vp]),
+        "bfam_gpu_domain_launch_levels": (C.c_int, [vp]),
         "bfam_gpu_batch_num_groups": (C.c_int, [vp]),
         "bfam_gpu_batch_group_info": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int),
                                                 P(C.c_int), P(C.c_int64)]),
@@ -394,6 +396,10 @@ class GpuDomain:
     def device_bytes(self) -> int:
         return int(lib().bfam_gpu_domain_device_bytes(self._h))
 
+    def launch_levels(self) -> int:
+        """launches per LSRK stage (one per refinement level)"""
+        return int(lib().bfam_gpu_domain_launch_levels(self._h))
+
     def set_fields(self, q: np.ndarray) -> None:
         q = np.ascontiguousarray(q, dtype=np.float64)
         assert q.shape == (self.nfields, self.field_length)
@@ -513,6 +519,9 @@ class Batch:
             out.append({"dim": d.value, "N": n.value, "precision": p.value,
                         "elements": k.value})
         return out
+
+    def launches_per_step(self) -> int:
+        return int(lib().bfam_gpu_batch_launches_per_step(self._h))
 
     def set_tile(self, group: int, tile: int, ctas_per_sm: int = 0) -> None:
         _check(lib().bfam_gpu_batch_set_tile(self._h, group, tile, ctas_per_sm))

@@ -14,6 +14,7 @@
 #include "dg_stage.cuh"
 #include "gpu_internal.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -243,10 +244,13 @@ struct bfam_gpu_batch
     std::vector<int> doms; // indices into the batch's domain list
     std::vector<double> hops;
     std::vector<BatchTile> tiles;
-    int tile = 0, ctas_per_sm = 0, grid = 0;
-    int64_t nwork = 0;
+    int tile = 0, ctas_per_sm = 0;
+    int64_t nwork = 0; // elements of all levels
     DomainView *views[2] = {nullptr, nullptr}; // per batch parity
-    int2 *work = nullptr;
+    // per launch level: (domain, element) work list, its length and grid
+    std::vector<int2 *> work;
+    std::vector<int64_t> nwork_l;
+    std::vector<int> grid;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
   };
@@ -333,7 +337,9 @@ int choose_grid(bfam_gpu_batch_t *b, bfam_gpu_batch_t::Group &g)
   const int per_sm = g.ctas_per_sm > 0 && g.ctas_per_sm < occ ? g.ctas_per_sm
                                                                : occ;
   const int64_t full = (int64_t)per_sm * b->sms;
-  g.grid = (int)(g.nwork < full ? g.nwork : full);
+  g.grid.resize(g.nwork_l.size());
+  for (size_t l = 0; l < g.nwork_l.size(); ++l)
+    g.grid[l] = (int)(g.nwork_l[l] < full ? g.nwork_l[l] : full);
   return 0;
 }
 
@@ -396,10 +402,15 @@ int issue_step(bfam_gpu_batch_t *b, int p)
       sp.C = b->C[s];
       sp.first_stage = s == 0;
       sp.flux = g.flux;
-      t.launch(g.views[(p + s) & 1], g.work, (int)g.nwork, sp, g.hops.data(),
-               g.grid, g.stream);
-      CUDA_TRY(cudaGetLastError());
-      ++launches;
+      // levels in order: coarse elements after the fine ones across their
+      // hanging faces
+      for (size_t l = 0; l < g.work.size(); ++l)
+      {
+        t.launch(g.views[(p + s) & 1], g.work[l], (int)g.nwork_l[l], sp,
+                 g.hops.data(), g.grid[l], g.stream);
+        CUDA_TRY(cudaGetLastError());
+        ++launches;
+      }
     }
     CUDA_TRY(cudaEventRecord(g.done, g.stream));
     CUDA_TRY(cudaStreamWaitEvent(b->stream, g.done, 0));
@@ -414,7 +425,10 @@ int issue_step(bfam_gpu_batch_t *b, int p)
 
 int launches_per_step(const bfam_gpu_batch_t *b)
 {
-  return (int)b->groups.size() * b->ns + 1;
+  int n = 1;
+  for (const auto &g : b->groups)
+    n += b->ns * (int)g.work.size();
+  return n;
 }
 
 } // namespace
@@ -662,14 +676,35 @@ int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
       return fail(BFAM_GPU_EINVAL, "group of order %d has %lld elements",
                   G.N, (long long)G.nwork);
     }
-    std::vector<int2> work;
-    work.reserve(G.nwork);
-    for (size_t k = 0; k < G.doms.size(); ++k)
-      for (int32_t e = 0; e < doms[G.doms[k]]->K; ++e)
-        work.push_back(make_int2((int)k, e));
-    TRY(batch_alloc(b, (void **)&G.work, work.size() * sizeof(int2)));
-    CTRY(cudaMemcpy(G.work, work.data(), work.size() * sizeof(int2),
-                    cudaMemcpyHostToDevice));
+    int nl = 1;
+    for (int i : G.doms)
+      nl = std::max(nl, doms[i]->nlevels);
+    for (int l = 0; l < nl; ++l)
+    {
+      // level l of every domain, domain-major
+      std::vector<int2> work;
+      for (size_t k = 0; k < G.doms.size(); ++k)
+      {
+        const bfam_gpu_domain_t *d = doms[G.doms[k]];
+        if (d->nlevels == 1)
+        {
+          if (l == 0)
+            for (int32_t e = 0; e < d->K; ++e)
+              work.push_back(make_int2((int)k, e));
+        }
+        else if (l < d->nlevels)
+          for (int32_t j = d->level_off[l]; j < d->level_off[l + 1]; ++j)
+            work.push_back(make_int2((int)k, d->helist[j]));
+      }
+      if (work.empty())
+        continue;
+      int2 *dw = nullptr;
+      TRY(batch_alloc(b, (void **)&dw, work.size() * sizeof(int2)));
+      CTRY(cudaMemcpy(dw, work.data(), work.size() * sizeof(int2),
+                      cudaMemcpyHostToDevice));
+      G.work.push_back(dw);
+      G.nwork_l.push_back((int64_t)work.size());
+    }
     for (int p = 0; p < 2; ++p)
       TRY(batch_alloc(b, (void **)&G.views[p],
                       G.doms.size() * sizeof(DomainView)));
@@ -828,6 +863,11 @@ int bfam_gpu_batch_sync(bfam_gpu_batch_t *b)
       return rc;
   }
   return 0;
+}
+
+int bfam_gpu_batch_launches_per_step(const bfam_gpu_batch_t *b)
+{
+  return b ? launches_per_step(b) : 0;
 }
 
 int bfam_gpu_batch_free(bfam_gpu_batch_t *b)

@@ -9,6 +9,7 @@
 #include "dg_stage.cuh"
 #include "gpu_internal.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -48,17 +49,17 @@ namespace
 
 template <int DIM, int N, typename CT>
 void stage_launch(const DomainView &v, const StageParams &sp,
-                  const double *hops, int mode, cudaStream_t stream)
+                  const double *hops, int mode, int grid, cudaStream_t stream)
 {
   using S = Shape<DIM, N>;
   const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
   const size_t smem = stage_smem_bytes<DIM, N, CT>();
   if (mode == MODE_STAGE)
     dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>
-        <<<v.K, S::NT, smem, stream>>>(v, sp, dop);
+        <<<grid, S::NT, smem, stream>>>(v, sp, dop);
   else
     dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_RHS, CT>
-        <<<v.K, S::NT, smem, stream>>>(v, sp, dop);
+        <<<grid, S::NT, smem, stream>>>(v, sp, dop);
 }
 
 template <typename K> cudaError_t allow_smem(K kernel, int bytes)
@@ -233,9 +234,10 @@ DomainView view(bfam_gpu_domain_t *d, int in)
   v.rhs = d->rhs;
   v.ed = d->ed;
   v.fdesc = d->fdesc;
-  v.gpart = d->gpart;
   v.fcE = d->fcE;
-  v.fcG = d->fcG;
+  v.fslot = d->fslot;
+  v.mbuf = d->mbuf;
+  v.elist = nullptr;
   v.ops = d->ops;
   v.err = d->err;
   v.dt = 0;
@@ -256,9 +258,21 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double C,
   sp.flux = d->flux;
   DomainView v = view(d, in);
   v.dt = dt;
-  d->ks.launch(v, sp, d->hops.data(), mode, d->stream);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
-  CUDA_TRY(cudaGetLastError());
+  // one launch per level; level l's elements after level l-1's
+  for (int l = 0; l < d->nlevels; ++l)
+  {
+    int grid = d->K;
+    if (d->nlevels > 1)
+    {
+      v.elist = d->elist + d->level_off[l];
+      grid = d->level_off[l + 1] - d->level_off[l];
+    }
+    if (grid == 0)
+      continue;
+    d->ks.launch(v, sp, d->hops.data(), mode, grid, d->stream);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    CUDA_TRY(cudaGetLastError());
+  }
   return 0;
 }
 
@@ -430,8 +444,17 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
                   "element",
                   i / NF, i % NF);
 
+  // ---- mortar buffer slots: one per coarse-side glue element (piece), in
+  // glue order, so that a coarse face's pieces have consecutive slots
+  std::vector<int32_t> mslot(Kg > 0 ? Kg : 1, -1);
+  int32_t nslot = 0;
+  for (int32_t g = 0; g < Kg; ++g)
+    if (glue->EToHm[g] > 0)
+      mslot[g] = nslot++;
+
   // ---- compact descriptors read by the kernel (layout in dg_common.cuh)
   std::vector<int2> fdesc((size_t)K * NF);
+  std::vector<int32_t> fslot((size_t)K * NF, -1);
   for (size_t i = 0; i < fdesc.size(); ++i)
   {
     const int32_t nb = nbr[i];
@@ -448,17 +471,55 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
       fdesc[i] = make_int2(glue->EToEm[pg], 1 | (glue->EToFm[pg] << 2) |
                                                 (glue->EToOp[g0] << 5) |
                                                 (glue->EToHm[pg] << 8));
+      if (glue->EToHm[pg] > 0)
+        fslot[i] = mslot[pg];
     }
     else
-      fdesc[i] = make_int2(g0, 2);
+      fdesc[i] = make_int2(mslot[g0], 2);
   }
-  std::vector<int2> gpart(Kg > 0 ? Kg : 1, make_int2(0, 0));
-  for (int32_t g = 0; g < Kg; ++g)
+
+  // ---- launch levels: an element with coarse faces runs after the fine
+  // elements across them (which write its mortar slots); level 0 has no
+  // coarse face
+  std::vector<int> level(K, 0);
+  int nlevels = 1;
+  for (bool changed = Kg > 0; changed;)
   {
-    const int32_t pg = glue->EToEp[g];
-    gpart[g] = make_int2(glue->EToEm[pg], glue->EToFm[pg] |
-                                              (glue->EToOp[g] << 3) |
-                                              (glue->EToHm[g] << 6));
+    changed = false;
+    for (int32_t e = 0; e < K; ++e)
+      for (int f = 0; f < NF; ++f)
+      {
+        const int2 ds = fdesc[(size_t)e * NF + f];
+        if ((ds.y & 3) != 2)
+          continue;
+        const int32_t g0 = -1 - nbr[(size_t)e * NF + f];
+        for (int p = 0; p < NPc; ++p)
+        {
+          const int32_t fine = glue->EToEm[glue->EToEp[g0 + p]];
+          if (level[e] < level[fine] + 1)
+          {
+            level[e] = level[fine] + 1;
+            changed = true;
+            if (level[e] >= K)
+              return fail(BFAM_GPU_EINVAL,
+                          "hanging faces form a cycle (element %d)", e);
+          }
+        }
+      }
+  }
+  for (int32_t e = 0; e < K; ++e)
+    nlevels = std::max(nlevels, level[e] + 1);
+  std::vector<int32_t> elist, level_off(nlevels + 1, 0);
+  if (nlevels > 1)
+  {
+    for (int32_t e = 0; e < K; ++e)
+      ++level_off[level[e] + 1];
+    for (int l = 0; l < nlevels; ++l)
+      level_off[l + 1] += level_off[l];
+    elist.resize(K);
+    std::vector<int32_t> pos(level_off.begin(), level_off.end() - 1);
+    for (int32_t e = 0; e < K; ++e)
+      elist[pos[level[e]]++] = e;
   }
 
   // ---- operators: Dr | interp[3] | proj[3] | w
@@ -539,9 +600,6 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
   for (size_t i = 0; i < fcE.size(); ++i)
     if ((fdesc[i].y & 3) != 2)
       fcE[i] = fconst((int32_t)(i / NF), fdesc[i].x);
-  std::vector<double4> fcG(Kg > 0 ? Kg : 1, make_double4(0, 0, 0, 0));
-  for (int32_t g = 0; g < Kg; ++g)
-    fcG[g] = fconst(glue->EToEm[g], glue->EToEm[glue->EToEp[g]]);
 
   // ---- device
   bfam_gpu_domain_t *d = new bfam_gpu_domain_t();
@@ -603,9 +661,18 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
   TRY(dev_alloc(d, (void **)&d->dq, state));
   TRY(upload(d, &d->ed, ed.data(), ed.size()));
   TRY(upload(d, &d->fdesc, fdesc.data(), fdesc.size()));
-  TRY(upload(d, &d->gpart, gpart.data(), gpart.size()));
   TRY(upload(d, &d->fcE, fcE.data(), fcE.size()));
-  TRY(upload(d, &d->fcG, fcG.data(), fcG.size()));
+  if (nslot > 0)
+  {
+    TRY(upload(d, &d->fslot, fslot.data(), fslot.size()));
+    TRY(dev_alloc(d, (void **)&d->mbuf,
+                  sizeof(double) * (size_t)nslot * 2 * dim * Nfp));
+  }
+  d->nlevels = nlevels;
+  d->level_off = level_off;
+  if (nlevels > 1)
+    TRY(upload(d, &d->elist, elist.data(), elist.size()));
+  d->helist = elist;
   TRY(upload(d, &d->ops, ops.data(), ops.size()));
   TRY(dev_alloc(d, (void **)&d->err, sizeof(int)));
   TRY(dev_alloc(d, (void **)&d->clock, sizeof(DomainClock)));
@@ -627,6 +694,11 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
   (void)nmap;
   *out = d;
   return 0;
+}
+
+int bfam_gpu_domain_launch_levels(const bfam_gpu_domain_t *d)
+{
+  return d ? d->nlevels : 0;
 }
 
 int bfam_gpu_domain_free(bfam_gpu_domain_t *d)
@@ -916,7 +988,7 @@ int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
     }
     return post ? launch_post(d, in, dt) : 0;
   };
-  const int per_step = ts->ns + (post ? 1 : 0);
+  const int per_step = ts->ns * d->nlevels + (post ? 1 : 0);
   for (int st = 0; st < nsteps; ++st)
   {
     const int c0 = d->cur;

@@ -22,10 +22,10 @@ struct ElemData
 //   1 glue, whole face:  a = partner element (same size or coarse),
 //                        b>>2 & 7 = partner face, b>>5 & 7 = glue orientation,
 //                        b>>8 & 7 = partner's hanging piece (0: same size)
-//   2 glue, coarse side: a = first of the face's glue elements
-// Glue partner, one per glue element g (used on the coarse side):
-//   a = partner (fine) element, b & 7 = partner face, b>>3 & 7 = orientation,
-//   b>>6 & 7 = hanging piece of g.
+//   2 glue, coarse side: a = mortar buffer slot of the face's first piece
+//                        (the pieces' slots are consecutive, in glue order)
+// A fine face (kind 1 with a hanging piece) writes its projected coarse-side
+// jumps to mortar slot fslot[e][f].
 // Per-domain clock in device memory, advanced once per time step by the
 // post-step kernel, so that replayed CUDA graphs see the current time.
 struct DomainClock
@@ -56,11 +56,12 @@ struct DomainView
   double *__restrict__ rhs; // right-hand-side output (rhs mode)
   const ElemData *__restrict__ ed;
   const int2 *__restrict__ fdesc; // [K][NF]
-  const int2 *__restrict__ gpart; // [Kg]
   // upwind flux constants {Zp+, 1/(Zp- + Zp+), Zs+, 1/(Zs- + Zs+)}:
   const double4 *__restrict__ fcE; // [K][NF] conforming / whole-face glue
-  const double4 *__restrict__ fcG; // [Kg] per glue element (coarse side)
-  const double *__restrict__ ops;  // Dr | interp[3] | proj[3] | w
+  const int *__restrict__ fslot;   // [K][NF] mortar slot of a fine face
+  double *mbuf; // [slots][NJ][Nfp] projected coarse-side jumps per piece
+  const int *__restrict__ elist; // elements of this launch (NULL: all)
+  const double *__restrict__ ops; // Dr | interp[3] | proj[3] | w
   int *err;
   double dt; // time step of this domain (batches step domains with their own)
   PointSource src;
@@ -135,15 +136,15 @@ template <int DIM, int N> struct Shape
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q
   static constexpr int SM_DQ = SM_QS; // dq, then A dq + dt rhs in place
   static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
-  static constexpr int SM_OI = NPC * NTF * Nfp + (NPC * NTF * Nfp) % 2;
-  // mortar scratch: own trace on the pieces, fine partners' traces
-  static constexpr int SM_MOR = 2 * SM_OI;
-  // face and piece flux constants, then the element record (ElemData)
-  static constexpr int SM_FC = 4 * (NF + NPC) + 8;
-  // differentiation matrix
-  static constexpr int SM_IP = Nq * Nq + (Nq % 2);
+  // coarse-side jumps of the fine faces, projected in place
+  static constexpr int SM_MJ = NF * NJ * Nfp + (NF * NJ * Nfp) % 2;
+  // face flux constants, then the element record (ElemData)
+  static constexpr int SM_FC = 4 * NF + 8;
+  // differentiation matrix, bottom-half mortar interpolation and projection
+  // (Nq*Nq entries each, one double slot per entry)
+  static constexpr int SM_IP = 3 * Nq * Nq + (Nq % 2);
   static constexpr int SM_TOTAL =
-      SM_QS + SM_DQ + SM_PT + SM_MOR + SM_FC + SM_IP + 4;
+      SM_QS + SM_DQ + SM_PT + SM_MJ + SM_FC + SM_IP + 4;
   // precision form only: FP32 copy of q minus the element's first node,
   // after the mbarriers
   static constexpr int SM_QF = (NFLD * Np + 3) / 4 * 2;
@@ -389,6 +390,50 @@ __device__ __forceinline__ void apply_half(const DiffOp<N, CT> &op, int top,
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
     out[m] = top ? o[N - m] : o[m];
+}
+
+// out = A v with A(m, i) = A[m + Nq i] a bottom-half mortar operator held in
+// shared memory (AT: its stored type), or its top-half reflection when
+// top != 0 (see apply_half).
+template <int N, typename T, typename AT>
+__device__ __forceinline__ void apply_half_s(const AT *A, int top, const T *v,
+                                             T *out)
+{
+  constexpr int Nq = N + 1;
+  T vr[Nq], o[Nq];
+#pragma unroll
+  for (int i = 0; i < Nq; ++i)
+    vr[i] = top ? v[N - i] : v[i];
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+  {
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < Nq; ++i)
+      s += T(A[m + Nq * i]) * vr[i];
+    o[m] = s;
+  }
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+    out[m] = top ? o[N - m] : o[m];
+}
+
+// line_apply with the operator in shared memory (OFFSET: interpolate the
+// variation along the line, as line_apply does for narrow types)
+template <int N, bool OFFSET, typename T, typename AT>
+__device__ __forceinline__ void line_apply_s(const AT *A, int top, double *x,
+                                             int stride)
+{
+  constexpr int Nq = N + 1;
+  const double ref = OFFSET ? x[0] : 0.0;
+  T v[Nq];
+#pragma unroll
+  for (int i = 0; i < Nq; ++i)
+    v[i] = OFFSET ? T(x[i * stride] - ref) : T(x[i * stride]);
+  apply_half_s<N, T, AT>(A, top, v, v);
+#pragma unroll
+  for (int m = 0; m < Nq; ++m)
+    x[m * stride] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
 // In-place 1-D mortar operator pass on one line of a face array

@@ -14,12 +14,14 @@
 //             fine side of hanging faces), lifted with the lumped LGL mass to
 //             per-node field contributions;
 //   mortar  : faces that go through the glue grid (2:1 hanging faces,
-//             src/bfam.c:7328-7520): on the fine side the coarse neighbour's
-//             trace is interpolated to this element's mortar piece
-//             (interpolation[1..2]); on the coarse side the element's own trace
-//             is interpolated to the four (2D: two) pieces, the flux evaluated
-//             there against each fine neighbour and L2-projected back
-//             (projection[1..2]) -- all pieces of a face at once;
+//             src/bfam.c:7328-7520).  The fine element interpolates the coarse
+//             neighbour's trace to its mortar piece (interpolation[1..2]) and
+//             evaluates the flux there; from the same Riemann solution it
+//             forms the coarse side's jumps on the piece, L2-projects them to
+//             the coarse face (projection[1..2]) and stores them in a mortar
+//             buffer slot.  The coarse element, launched after its fine
+//             neighbours (elements are launched by level), sums its pieces'
+//             projected jumps and lifts them;
 //   volume  : one thread per node, the tensor-product LGL derivative along each
 //             axis (the BFAM_KRON_IXIXA / IXAXI / AXIXI contractions of
 //             src/bfam.c:3519-3624 at one node), plus the node's face
@@ -46,165 +48,12 @@
 namespace bfam_b200
 {
 
-// Fine partners' traces (the NTF trace fields of face axis ax) and flux
-// constants of one coarse-side glue face, glue elements g0 .. g0 + NPC - 1,
-// gathered into ms / fcp with cp.async (the caller commits the group).
-template <int DIM, int N, int NT>
-__device__ __forceinline__ void
-issue_partners(const double *__restrict__ qin, size_t fs,
-               const int2 *__restrict__ gpart, const double4 *__restrict__ fcG,
-               int g0, int ax, double *ms, double *fcp)
+// index of the i-th set bit of m
+__device__ __forceinline__ int nth_bit(int m, int i)
 {
-  using S = Shape<DIM, N>;
-  constexpr int Np = S::Np, Nfp = S::Nfp, NPC = S::NPC, NTF = S::NTF;
-  for (int w = threadIdx.x; w < NPC * Nfp; w += NT)
-  {
-    const int p = w / Nfp, pn = w % Nfp;
-    const int2 gp = gpart[g0 + p];
-    const double *src = qin + (size_t)gp.x * Np + gmask<DIM, N>(gp.y & 7, pn);
-    double *dst = ms + p * NTF * Nfp + pn;
-#pragma unroll
-    for (int c = 0; c < NTF; ++c)
-      cp_async8(dst + c * Nfp, src + trace_field<DIM>(ax, c) * fs);
-    if (pn == 0)
-    {
-      const double *fc = reinterpret_cast<const double *>(fcG + g0 + p);
-      cp_async16(fcp + 4 * p, fc);
-      cp_async16(fcp + 4 * p + 2, fc + 2);
-    }
-  }
-}
-
-// Coarse side of glue face f (glue elements g0 .. g0 + NPC - 1): the
-// element's own trace interpolated to the NPC pieces, the flux against each
-// fine partner there, the jumps L2-projected back (FP64), summed and lifted
-// into pt.  When fnext >= 0 the next coarse face's partners (from gnext) are
-// fetched as soon as ms is free.  Kept out of line: few elements have a
-// coarse face, and inlined its register demand adds to the volume pass's.
-template <int DIM, int N, int NT, typename CT>
-__device__ __noinline__ void
-coarse_face(const double *__restrict__ qin, size_t fs,
-            const int2 *__restrict__ gpart, const double4 *__restrict__ fcG,
-            const DiffOp<N, CT> *dop, int f, int g0, int fnext, int gnext,
-            int flux, double s)
-{
-  using S = Shape<DIM, N>;
-  constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
-                NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
-                NTF = S::NTF;
-  extern __shared__ __align__(16) double smem[];
-  double *qs = smem;
-  double *pt = qs + S::SM_QS + S::SM_DQ;
-  double *oi = pt + S::SM_PT;
-  double *ms = oi + S::SM_OI;
-  double *fcp = oi + S::SM_MOR + 4 * NF;
-  const ElemData &me = *reinterpret_cast<const ElemData *>(fcp + 4 * NPC);
-  const int t = threadIdx.x;
-  auto lfac = [&](int ax) {
-    return CT(s * (ax == 0 ? me.rx : (ax == 1 ? me.ry : me.rz)) * dop->iwend);
-  };
-  cp_async_wait<0>();
-  __syncthreads(); // ms holds this face's partners; oi is free
-  // own face trace -> pieces, along face axis 0
-  for (int w = t; w < NPC * NTF * ROWS; w += NT)
-  {
-    const int p = w / (NTF * ROWS), r = w % (NTF * ROWS);
-    const int c = r / ROWS, line = r % ROWS;
-    const int h = (gpart[g0 + p].y >> 6) & 7;
-    // face line `line` is an arithmetic run of volume nodes
-    const double *src = qs + trace_field<DIM>(f >> 1, c) * Np +
-                        gmask<DIM, N>(f, Nq * line);
-    const int st = gmask<DIM, N>(f, 1) - gmask<DIM, N>(f, 0);
-    // narrower than double: interpolate the variation along the line
-    constexpr bool OFFSET = sizeof(CT) < sizeof(double);
-    const double ref = OFFSET ? src[0] : 0.0;
-    CT v[Nq];
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-      v[i] = OFFSET ? CT(src[st * i] - ref) : CT(src[st * i]);
-    apply_half<N, false, CT, CT>(*dop, (h - 1) & 1, v, v);
-    double *x = oi + (p * NTF + c) * Nfp + Nq * line;
-#pragma unroll
-    for (int m = 0; m < Nq; ++m)
-      x[m] = OFFSET ? ref + double(v[m]) : double(v[m]);
-  }
-  __syncthreads();
-  if (DIM == 3)
-  {
-    for (int w = t; w < NPC * NTF * Nq; w += NT)
-    {
-      const int p = w / (NTF * Nq), r = w % (NTF * Nq);
-      const int c = r / Nq, col = r % Nq;
-      const int h = (gpart[g0 + p].y >> 6) & 7;
-      line_apply<N, false, CT, CT>(*dop, (h - 1) >> 1,
-                                   oi + (p * NTF + c) * Nfp + col, Nq);
-    }
-    __syncthreads();
-  }
-  // flux on the pieces; jumps overwrite the own trace in place
-  for (int w = t; w < NPC * Nfp; w += NT)
-  {
-    const int p = w / Nfp, pn = w % Nfp;
-    const int pp = map_op<DIM, N>((gpart[g0 + p].y >> 3) & 7, pn);
-    CT dq[NTF], J[6];
-    double *x = oi + p * NTF * Nfp;
-    const double *y = ms + p * NTF * Nfp;
-#pragma unroll
-    for (int c = 0; c < NTF; ++c)
-      dq[c] = CT(y[c * Nfp + pp] - x[c * Nfp + pn]);
-    flux_jumps<DIM, CT>(dq, f >> 1, (f & 1) ? CT(1) : CT(-1), CT(me.Zp),
-                        CT(me.Zs), fcp + 4 * p, flux, J);
-#pragma unroll
-    for (int c = 0; c < NJ; ++c)
-      x[c * Nfp + pn] = double(J[jslot<DIM>(c)]);
-  }
-  __syncthreads(); // ms and fcp free: fetch the next face's partners
-  if (fnext >= 0)
-  {
-    issue_partners<DIM, N, NT>(qin, fs, gpart, fcG, gnext, fnext >> 1, ms,
-                               fcp);
-    cp_async_commit();
-  }
-  // L2 projection back to the coarse face (FP64): axis 0, (axis 1), sum
-  for (int w = t; w < NPC * NJ * ROWS; w += NT)
-  {
-    const int p = w / (NJ * ROWS), r = w % (NJ * ROWS);
-    const int c = r / ROWS, line = r % ROWS;
-    const int h = (gpart[g0 + p].y >> 6) & 7;
-    line_apply<N, true, double, CT>(*dop, (h - 1) & 1,
-                                    oi + (p * NTF + c) * Nfp + Nq * line, 1);
-  }
-  __syncthreads();
-  if (DIM == 3)
-  {
-    for (int w = t; w < NPC * NJ * Nq; w += NT)
-    {
-      const int p = w / (NJ * Nq), r = w % (NJ * Nq);
-      const int c = r / Nq, col = r % Nq;
-      const int h = (gpart[g0 + p].y >> 6) & 7;
-      line_apply<N, true, double, CT>(*dop, (h - 1) >> 1,
-                                      oi + (p * NTF + c) * Nfp + col, Nq);
-    }
-    __syncthreads();
-  }
-  for (int pn = t; pn < Nfp; pn += NT)
-  {
-    CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
-#pragma unroll
-    for (int c = 0; c < NJ; ++c)
-    {
-      double sum = 0;
-#pragma unroll
-      for (int p = 0; p < NPC; ++p)
-        sum += oi[(p * NTF + c) * Nfp + pn];
-      J[jslot<DIM>(c)] = CT(sum);
-    }
-    lift_face<DIM, CT>(J, f >> 1, (f & 1) ? CT(1) : CT(-1), lfac(f >> 1), me,
-                       lc);
-#pragma unroll
-    for (int c = 0; c < NFLD; ++c)
-      pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
-  }
+  for (; i > 0; --i)
+    m &= m - 1;
+  return __ffs(m) - 1;
 }
 
 // One element of one stage.  `iter` counts the elements this CTA has done
@@ -217,20 +66,21 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
 {
   using S = Shape<DIM, N>;
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
-                NFLD = S::NFLD, NPC = S::NPC, ROWS = S::ROWS, NTF = S::NTF;
+                NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
+                NTF = S::NTF;
   static_assert(NT >= NF * Nfp, "one face-node work item per thread");
   // the dynamic shared array itself (not a pointer parameter), so that all
   // accesses stay in the shared window with 32-bit addressing
   extern __shared__ __align__(16) double smem[];
   double *qs = smem;
-  double *R = qs + S::SM_QS;    // dq tile
-  double *pt = R + S::SM_DQ;    // [NF][NFLD][Nfp] plus traces, then lifted
-  double *oi = pt + S::SM_PT;   // [NPC][NTF][Nfp] own trace on mortar pieces
-  double *ms = oi + S::SM_OI;   // [NPC][NTF][Nfp] fine partners' traces
-  double *fcf = oi + S::SM_MOR; // [NF][4] face flux constants
-  double *fcp = fcf + 4 * NF;   // [NPC][4] piece flux constants
-  double *sE = fcp + 4 * NPC;   // element record
+  double *R = qs + S::SM_QS;   // dq tile
+  double *pt = R + S::SM_DQ;   // [NF][NFLD][Nfp] plus traces, then lifted
+  double *mj = pt + S::SM_PT;  // [NF][NJ][Nfp] coarse-side jumps of fine faces
+  double *fcf = mj + S::SM_MJ; // [NF][4] face flux constants
+  double *sE = fcf + 4 * NF;   // element record
   CT *sD = reinterpret_cast<CT *>(sE + 8); // differentiation matrix
+  CT *sIb = reinterpret_cast<CT *>(sE + 8 + Nq * Nq); // mortar operators
+  double *sPb = sE + 8 + 2 * Nq * Nq;
   uint64_t *bar = reinterpret_cast<uint64_t *>(sE + 8 + S::SM_IP);
   // the volume pass's copy of q: q itself in the plain form; in the
   // precision form FP32 q minus the element's first node per field (the
@@ -264,6 +114,7 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
     fine_mask |= ((y & 3) == 1 && ((y >> 8) & 7) != 0) << f;
     permuted |= (y & 3) == 1 && ((y >> 5) & 7) != 0;
   }
+  const int ncoarse = __popc(coarse_mask), nfine = __popc(fine_mask);
 
   // ---------------------------------------------------------- phase 0: issue
   if constexpr (S::TMA)
@@ -295,7 +146,6 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
         cp_async8(R + w, d.dq + (w / Np) * fs + eoff + (w % Np));
     }
   }
-  cp_async_commit(); // own state (non-TMA path)
 
   // neighbour traces of conforming faces and coarse partners of fine-side
   // glue faces, gathered into pt in this element's face-node order
@@ -326,17 +176,15 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   if (t < 4)
     cp_async16(sE + 2 * t,
                reinterpret_cast<const double *>(d.ed + e) + 2 * t);
-  cp_async_commit(); // face traces, flux constants, element record
+  cp_async_commit(); // own state (non-TMA path), face traces, constants
 
-  int next_coarse = coarse_mask ? __ffs(coarse_mask) - 1 : -1;
-  if (next_coarse >= 0)
-    issue_partners<DIM, N, NT>(d.qin, fs, d.gpart, d.fcG, desc[next_coarse].x,
-                               next_coarse >> 1, ms, fcp);
-  cp_async_commit(); // fine partners (possibly empty)
-
-  // differentiation matrix into shared memory (indexed per thread later)
+  // 1-D operators into shared memory (indexed per thread later)
   for (int w = t; w < Nq * Nq; w += NT)
+  {
     sD[w] = dop.D[w];
+    sIb[w] = dop.Ib[w];
+    sPb[w] = dop.Pb[w];
+  }
 
   // ------------------------------------------------- phase 1: faces, mortars
   if constexpr (S::TMA)
@@ -344,7 +192,7 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
     if (!mbar_wait(&bar[0], par))
       atomicExch(d.err, 1);
   }
-  cp_async_wait<1>(); // own state (non-TMA path), face traces
+  cp_async_wait<0>();
   if constexpr (NARROW && !S::TMA)
     __syncthreads(); // other threads' cp.async writes of q
   if constexpr (NARROW)
@@ -359,15 +207,14 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   };
 
   // fine side: coarse partner trace -> my piece, in place (rows, then columns)
-  if (fine_mask)
+  if (nfine)
   {
     for (int pass = 0; pass < (DIM == 3 ? 2 : 1); ++pass)
     {
-      for (int w = t; w < NF * NTF * ROWS; w += NT)
+      for (int w = t; w < nfine * NTF * ROWS; w += NT)
       {
-        const int f = w / (NTF * ROWS), r = w % (NTF * ROWS);
-        if (!((fine_mask >> f) & 1))
-          continue;
+        const int f = nth_bit(fine_mask, w / (NTF * ROWS)),
+                  r = w % (NTF * ROWS);
         const int hp = (desc[f].y >> 8) & 7;
         const int c = r / ROWS, line = r % ROWS;
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
@@ -384,7 +231,12 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   // flux on conforming and fine-side faces, lifted to the face node's field
   // contributions, written in place over the node's own trace slots.  A
   // thread reads only its own node's slots unless a glue face permutes its
-  // partner's nodes; only then are all reads finished before any write.
+  // partner's nodes; only then are all reads finished before any write.  On
+  // a fine face the coarse side's jumps follow from the same Riemann
+  // solution (star state v*, S* n shared by both sides, coarse normal -n):
+  //   coarse (T* - T-) = -(fine J_T) + [T],  coarse (v* - v-) = fine J_v - [v]
+  // with [.] = coarse - fine as seen from the fine side; they go to mj in the
+  // coarse piece's node order.
   {
     CT lc[NFLD];
     int my_f = -1, my_pn = 0;
@@ -407,6 +259,17 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
         const CT sg = (f & 1) ? CT(1) : CT(-1);
         flux_jumps<DIM, CT>(dq, f >> 1, sg, CT(me.Zp), CT(me.Zs),
                             fcf + 4 * f, sp.flux, J);
+        if ((fine_mask >> f) & 1)
+        {
+          double *m = mj + f * NJ * Nfp + pp;
+#pragma unroll
+          for (int c = 0; c < NJ; ++c)
+          {
+            const int sl = jslot<DIM>(c);
+            const CT v = sl < 3 ? sg * dq[DIM + sl] - J[sl] : J[sl] - dq[sl - 3];
+            m[c * Nfp] = double(v);
+          }
+        }
         lift_face<DIM, CT>(J, f >> 1, sg, lfac(f >> 1), me, lc);
         if (!permuted)
         {
@@ -428,16 +291,60 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
     }
   }
 
-  // coarse side: all pieces of one face at a time
-  while (next_coarse >= 0)
+  // coarse side: the pieces' projected jumps, summed in glue order, lifted
+  for (int w = t; w < ncoarse * Nfp; w += NT)
   {
-    const int f = next_coarse;
-    coarse_mask &= ~(1 << f);
-    next_coarse = coarse_mask ? __ffs(coarse_mask) - 1 : -1;
-    coarse_face<DIM, N, NT, CT>(d.qin, fs, d.gpart, d.fcG, &dop, f, desc[f].x,
-                                next_coarse,
-                                next_coarse >= 0 ? desc[next_coarse].x : 0,
-                                sp.flux, s);
+    const int f = nth_bit(coarse_mask, w / Nfp), pn = w % Nfp;
+    const double *mb = d.mbuf + (size_t)desc[f].x * NJ * Nfp + pn;
+    CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
+#pragma unroll
+    for (int c = 0; c < NJ; ++c)
+    {
+      double sum = 0;
+#pragma unroll
+      for (int p = 0; p < NPC; ++p)
+        sum += mb[(p * NJ + c) * Nfp];
+      J[jslot<DIM>(c)] = CT(sum);
+    }
+    lift_face<DIM, CT>(J, f >> 1, (f & 1) ? CT(1) : CT(-1), lfac(f >> 1), me,
+                       lc);
+#pragma unroll
+    for (int c = 0; c < NFLD; ++c)
+      pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
+  }
+
+  // fine side: L2 projection of the coarse-side jumps to the coarse face
+  // (FP64), then out to the mortar buffer for the coarse element
+  if (nfine)
+  {
+    __syncthreads();
+    for (int w = t; w < nfine * NJ * ROWS; w += NT)
+    {
+      const int f = nth_bit(fine_mask, w / (NJ * ROWS)), r = w % (NJ * ROWS);
+      const int hp = (desc[f].y >> 8) & 7;
+      const int c = r / ROWS, line = r % ROWS;
+      line_apply_s<N, false, double, double>(
+          sPb, (hp - 1) & 1, mj + (f * NJ + c) * Nfp + Nq * line, 1);
+    }
+    __syncthreads();
+    if (DIM == 3)
+    {
+      for (int w = t; w < nfine * NJ * Nq; w += NT)
+      {
+        const int f = nth_bit(fine_mask, w / (NJ * Nq)), r = w % (NJ * Nq);
+        const int hp = (desc[f].y >> 8) & 7;
+        const int c = r / Nq, col = r % Nq;
+        line_apply_s<N, false, double, double>(
+            sPb, (hp - 1) >> 1, mj + (f * NJ + c) * Nfp + col, Nq);
+      }
+      __syncthreads();
+    }
+    for (int w = t; w < nfine * NJ * Nfp; w += NT)
+    {
+      const int f = nth_bit(fine_mask, w / (NJ * Nfp)), r = w % (NJ * Nfp);
+      d.mbuf[(size_t)d.fslot[(size_t)e * NF + f] * NJ * Nfp + r] =
+          mj[f * NJ * Nfp + r];
+    }
   }
   __syncthreads();
 
@@ -538,7 +445,7 @@ __device__ __forceinline__ void stage_barriers_init(int offset)
 template <int DIM, int N> __host__ __device__ constexpr int bar_offset()
 {
   using S = Shape<DIM, N>;
-  return S::SM_QS + S::SM_DQ + S::SM_PT + S::SM_MOR + S::SM_FC + S::SM_IP;
+  return S::SM_QS + S::SM_DQ + S::SM_PT + S::SM_MJ + S::SM_FC + S::SM_IP;
 }
 
 // dynamic shared memory of one CTA of the stage kernel
@@ -550,14 +457,17 @@ __host__ __device__ constexpr size_t stage_smem_bytes()
          sizeof(double);
 }
 
-// One domain, one element per CTA.
+// One domain, one element per CTA: element blockIdx.x, or the
+// blockIdx.x-th of the launch's element list (meshes with hanging faces
+// launch their elements by level).
 template <int DIM, int N, int NT, int MINB, int MODE, typename CT>
 __global__ void __launch_bounds__(NT, MINB)
     dg_stage_kernel(DomainView d, StageParams sp,
                     const __grid_constant__ DiffOp<N, CT> dop)
 {
   stage_barriers_init(bar_offset<DIM, N>());
-  stage_element<DIM, N, NT, MODE, CT>(d, sp, dop, blockIdx.x, 0);
+  const int e = d.elist ? d.elist[blockIdx.x] : (int)blockIdx.x;
+  stage_element<DIM, N, NT, MODE, CT>(d, sp, dop, e, 0);
 }
 
 // Many domains of the same order in one persistent launch: CTAs stride over

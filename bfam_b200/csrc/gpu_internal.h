@@ -30,7 +30,8 @@ extern std::atomic<uint64_t> g_launches;
 
 // per-order launchers (the kernels' parameter lists depend on the order)
 typedef void (*stage_launch_fn)(const DomainView &, const StageParams &,
-                                const double *D, int mode, cudaStream_t);
+                                const double *D, int mode, int grid,
+                                cudaStream_t);
 typedef cudaError_t (*prepare_fn)();
 typedef void (*energy_fn)(const double *, size_t, const ElemData *,
                           const double *, double *);
@@ -82,9 +83,15 @@ struct bfam_gpu_domain
   double *energy = nullptr;
   bfam_b200::ElemData *ed = nullptr;
   int2 *fdesc = nullptr;
-  int2 *gpart = nullptr;
   double4 *fcE = nullptr;
-  double4 *fcG = nullptr;
+  int *fslot = nullptr;  // [K][NF] mortar slot of each fine face (-1: none)
+  double *mbuf = nullptr; // [slots][2 dim][Nfp] projected coarse-side jumps
+  // launch levels (meshes with hanging faces): elements of level l are
+  // elist[level_off[l] .. level_off[l+1])
+  int nlevels = 1;
+  std::vector<int32_t> level_off;
+  int32_t *elist = nullptr;
+  std::vector<int32_t> helist; // host copy of elist
   double *ops = nullptr;
   // host copy of Dr | interp[3] | proj[3] | w; the 1-D operators are passed
   // by value (kernel parameter bank) to each launch

@@ -190,6 +190,12 @@ int bfam_ts_lsrk_free(bfam_ts_lsrk_t *ts);
 /* Wait for the domain's stream and report device-side errors. */
 int bfam_gpu_domain_sync(bfam_gpu_domain_t *dom);
 
+/* Launches per LSRK stage (and per right-hand side): 1 for a conforming
+ * mesh; with 2:1 hanging faces one per refinement level, because an element
+ * with coarse-side hanging faces sums the projected mortar jumps that the
+ * fine elements across those faces produce earlier in the same stage. */
+int bfam_gpu_domain_launch_levels(const bfam_gpu_domain_t *dom);
+
 /* ------------------------------------------------------------------------
  * Point source and receivers (the serving requests' solves).  No
  * counterpart in the reference: bfam's DG path has no sources or receivers
@@ -255,6 +261,9 @@ int bfam_gpu_batch_step(bfam_gpu_batch_t *b, const double *dt, int nsteps,
 int bfam_gpu_batch_time(const bfam_gpu_batch_t *b, int i, double *t);
 /* Wait for the batch's stream and report device-side errors. */
 int bfam_gpu_batch_sync(bfam_gpu_batch_t *b);
+/* Kernel launches of one batch step (stage launches of every group and
+ * level, plus the post-step launch). */
+int bfam_gpu_batch_launches_per_step(const bfam_gpu_batch_t *b);
 int bfam_gpu_batch_free(bfam_gpu_batch_t *b);
 /* Number of order groups, and group g's (dim, N, precision, elements). */
 int bfam_gpu_batch_num_groups(const bfam_gpu_batch_t *b);

@@ -67,7 +67,12 @@ def test_batch_equals_each_domain_alone_and_the_oracle():
     n0 = bf.launch_count()
     b.step(dts, nsteps)
     b.sync()
-    assert bf.launch_count() - n0 == nsteps * (5 * len(groups) + 1)
+    per_step = b.launches_per_step()
+    # one launch per order group, refinement level and stage, plus post-step
+    lv = [d.launch_levels() for d in doms]
+    assert all(x == 2 for x in lv)  # every mesh here has hanging faces
+    assert per_step == 1 + 5 * 2 * len(groups)
+    assert bf.launch_count() - n0 == nsteps * per_step
     for i, ((m, rho, lam, mu, q0, dt), c) in enumerate(zip(probs, MIX)):
         got = doms[i].get_fields()
         alone, _ = _alone(m, rho, lam, mu, q0, dt, nsteps, c[5])
