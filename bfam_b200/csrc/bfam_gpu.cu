@@ -478,6 +478,20 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
       fdesc[i] = make_int2(mslot[g0], 2);
   }
 
+  // an element lies on the fine side of at most DIM hanging faces (the faces
+  // on its parent's boundary); the kernel's mortar scratch is sized for that
+  for (int32_t e = 0; e < K; ++e)
+  {
+    int nf = 0;
+    for (int f = 0; f < NF; ++f)
+      nf += fslot[(size_t)e * NF + f] >= 0;
+    if (nf > dim)
+      return fail(BFAM_GPU_EUNSUPPORTED,
+                  "element %d is on the fine side of %d hanging faces (a 2:1 "
+                  "balanced forest has at most %d)",
+                  e, nf, dim);
+  }
+
   // ---- launch levels: an element with coarse faces runs after the fine
   // elements across them (which write its mortar slots); level 0 has no
   // coarse face

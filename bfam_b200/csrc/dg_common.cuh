@@ -136,8 +136,10 @@ template <int DIM, int N> struct Shape
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q
   static constexpr int SM_DQ = SM_QS; // dq, then A dq + dt rhs in place
   static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
-  // coarse-side jumps of the fine faces, projected in place
-  static constexpr int SM_MJ = NF * NJ * Nfp + (NF * NJ * Nfp) % 2;
+  // coarse-side jumps of the fine faces, projected in place; an element has
+  // at most DIM faces on the fine side of a hanging face (those on its
+  // parent's boundary)
+  static constexpr int SM_MJ = DIM * NJ * Nfp + (DIM * NJ * Nfp) % 2;
   // face flux constants, then the element record (ElemData)
   static constexpr int SM_FC = 4 * NF + 8;
   // differentiation matrix, bottom-half mortar interpolation and projection

@@ -75,7 +75,7 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   double *qs = smem;
   double *R = qs + S::SM_QS;   // dq tile
   double *pt = R + S::SM_DQ;   // [NF][NFLD][Nfp] plus traces, then lifted
-  double *mj = pt + S::SM_PT;  // [NF][NJ][Nfp] coarse-side jumps of fine faces
+  double *mj = pt + S::SM_PT;  // [DIM][NJ][Nfp] coarse-side jumps, by fine rank
   double *fcf = mj + S::SM_MJ; // [NF][4] face flux constants
   double *sE = fcf + 4 * NF;   // element record
   CT *sD = reinterpret_cast<CT *>(sE + 8); // differentiation matrix
@@ -261,7 +261,9 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
                             fcf + 4 * f, sp.flux, J);
         if ((fine_mask >> f) & 1)
         {
-          double *m = mj + f * NJ * Nfp + pp;
+          // rank of f among the fine faces (an element has at most DIM)
+          const int fr = __popc(fine_mask & ((1 << f) - 1));
+          double *m = mj + fr * NJ * Nfp + pp;
 #pragma unroll
           for (int c = 0; c < NJ; ++c)
           {
@@ -320,30 +322,31 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
     __syncthreads();
     for (int w = t; w < nfine * NJ * ROWS; w += NT)
     {
-      const int f = nth_bit(fine_mask, w / (NJ * ROWS)), r = w % (NJ * ROWS);
-      const int hp = (desc[f].y >> 8) & 7;
+      const int fr = w / (NJ * ROWS), r = w % (NJ * ROWS);
+      const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
       const int c = r / ROWS, line = r % ROWS;
       line_apply_s<N, false, double, double>(
-          sPb, (hp - 1) & 1, mj + (f * NJ + c) * Nfp + Nq * line, 1);
+          sPb, (hp - 1) & 1, mj + (fr * NJ + c) * Nfp + Nq * line, 1);
     }
     __syncthreads();
     if (DIM == 3)
     {
       for (int w = t; w < nfine * NJ * Nq; w += NT)
       {
-        const int f = nth_bit(fine_mask, w / (NJ * Nq)), r = w % (NJ * Nq);
-        const int hp = (desc[f].y >> 8) & 7;
+        const int fr = w / (NJ * Nq), r = w % (NJ * Nq);
+        const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
         const int c = r / Nq, col = r % Nq;
         line_apply_s<N, false, double, double>(
-            sPb, (hp - 1) >> 1, mj + (f * NJ + c) * Nfp + col, Nq);
+            sPb, (hp - 1) >> 1, mj + (fr * NJ + c) * Nfp + col, Nq);
       }
       __syncthreads();
     }
     for (int w = t; w < nfine * NJ * Nfp; w += NT)
     {
-      const int f = nth_bit(fine_mask, w / (NJ * Nfp)), r = w % (NJ * Nfp);
+      const int fr = w / (NJ * Nfp), r = w % (NJ * Nfp);
+      const int f = nth_bit(fine_mask, fr);
       d.mbuf[(size_t)d.fslot[(size_t)e * NF + f] * NJ * Nfp + r] =
-          mj[f * NJ * Nfp + r];
+          mj[fr * NJ * Nfp + r];
     }
   }
   __syncthreads();
