@@ -37,7 +37,7 @@ typedef int (*batch_occupancy_fn)();
 
 struct BatchTile
 {
-  int NT = 0, MINB = 0;
+  int NT = 0, MINB = 0, NBUF = 1;
   batch_launch_fn launch = nullptr;
   batch_prepare_fn prepare = nullptr;
   batch_occupancy_fn occupancy = nullptr;
@@ -46,7 +46,8 @@ struct BatchTile
 template <int DIM, int N, int NT, int MINB, typename CT> struct TileImpl
 {
   static constexpr auto kernel =
-      dg_stage_batch_kernel<DIM, N, NT, MINB, MODE_STAGE, CT>;
+      dg_stage_batch_kernel<DIM, N, NT, MINB, MODE_STAGE, CT,
+                            nbuf<DIM, N, CT>()>;
   static void launch(const DomainView *v, const int2 *w, int nwork,
                      const StageParams &sp, const double *hops, int grid,
                      cudaStream_t st)
@@ -77,6 +78,7 @@ template <int DIM, int N, int NT, int MINB, typename CT> struct TileImpl
     BatchTile t;
     t.NT = NT;
     t.MINB = MINB;
+    t.NBUF = nbuf<DIM, N, CT>();
     t.launch = launch;
     t.prepare = prepare;
     t.occupancy = occupancy;
@@ -84,23 +86,24 @@ template <int DIM, int N, int NT, int MINB, typename CT> struct TileImpl
   }
 };
 
-// Tile shapes per order.  Tile 0 is the single-domain kernel's shape; the
-// others trade registers for resident CTAs (N = 3, 5) or threads for nodes
-// per thread (N = 7: 384 threads, one per face node, over 512 nodes).
+// Tile shapes per order.  Tile 0 is the single-domain kernel's shape (its
+// register budget sized for the CTAs the shared memory admits); the others
+// trade registers for resident CTAs or threads for nodes per thread (N = 7:
+// 384 threads, one per face node, over 512 nodes).
 template <typename CT> std::vector<BatchTile> tiles_for(int dim, int N)
 {
   std::vector<BatchTile> v;
 #define T(D, NN, NT, MB) v.push_back(TileImpl<D, NN, NT, MB, CT>::make())
-#define T0(D, NN) T(D, NN, (Shape<D, NN>::NT), (Shape<D, NN>::MINB))
+#define T0(D, NN) T(D, NN, (Shape<D, NN>::NT), (stage_min_ctas<D, NN, CT>()))
   if (dim == 3)
   {
     switch (N)
     {
     case 1: T0(3, 1); break;
     case 2: T0(3, 2); break;
-    case 3: T0(3, 3); T(3, 3, 96, 5); T(3, 3, 128, 5); break;
+    case 3: T0(3, 3); T(3, 3, 96, 4); T(3, 3, 128, 4); break;
     case 4: T0(3, 4); break;
-    case 5: T0(3, 5); T(3, 5, 224, 2); T(3, 5, 256, 2); break;
+    case 5: T0(3, 5); T(3, 5, 224, 1); T(3, 5, 256, 2); break;
     case 6: T0(3, 6); break;
     case 7: T0(3, 7); T(3, 7, 384, 1); break;
     default: break;
@@ -337,9 +340,12 @@ int choose_grid(bfam_gpu_batch_t *b, bfam_gpu_batch_t::Group &g)
   const int per_sm = g.ctas_per_sm > 0 && g.ctas_per_sm < occ ? g.ctas_per_sm
                                                                : occ;
   const int64_t full = (int64_t)per_sm * b->sms;
+  // a persistent grid for two-buffer tiles; one CTA per work item for
+  // one-buffer tiles
+  const bool persistent = t.NBUF == 2;
   g.grid.resize(g.nwork_l.size());
   for (size_t l = 0; l < g.nwork_l.size(); ++l)
-    g.grid[l] = (int)(g.nwork_l[l] < full ? g.nwork_l[l] : full);
+    g.grid[l] = (int)(persistent && g.nwork_l[l] > full ? full : g.nwork_l[l]);
   return 0;
 }
 

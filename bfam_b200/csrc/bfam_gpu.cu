@@ -47,19 +47,25 @@ int fail(int code, const char *fmt, ...)
 namespace
 {
 
+template <int DIM, int N, typename CT, int MODE>
+constexpr auto single_kernel =
+    dg_stage_kernel<DIM, N, Shape<DIM, N>::NT, stage_min_ctas<DIM, N, CT>(),
+                    MODE, CT, nbuf<DIM, N, CT>()>;
+
+// n work items on a persistent grid of `grid` CTAs
 template <int DIM, int N, typename CT>
-void stage_launch(const DomainView &v, const StageParams &sp,
+void stage_launch(const DomainView &v, int n, const StageParams &sp,
                   const double *hops, int mode, int grid, cudaStream_t stream)
 {
   using S = Shape<DIM, N>;
   const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
   const size_t smem = stage_smem_bytes<DIM, N, CT>();
   if (mode == MODE_STAGE)
-    dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>
-        <<<grid, S::NT, smem, stream>>>(v, sp, dop);
+    single_kernel<DIM, N, CT, MODE_STAGE><<<grid, S::NT, smem, stream>>>(
+        v, n, sp, dop);
   else
-    dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_RHS, CT>
-        <<<grid, S::NT, smem, stream>>>(v, sp, dop);
+    single_kernel<DIM, N, CT, MODE_RHS><<<grid, S::NT, smem, stream>>>(
+        v, n, sp, dop);
 }
 
 template <typename K> cudaError_t allow_smem(K kernel, int bytes)
@@ -69,16 +75,21 @@ template <typename K> cudaError_t allow_smem(K kernel, int bytes)
                               bytes);
 }
 
-template <int DIM, int N, typename CT> cudaError_t stage_prepare()
+// shared-memory opt-in, and the resident CTAs per SM of both modes
+template <int DIM, int N, typename CT> cudaError_t stage_prepare(int *occ)
 {
   using S = Shape<DIM, N>;
   const int smem = (int)stage_smem_bytes<DIM, N, CT>();
-  cudaError_t e = allow_smem(
-      dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_STAGE, CT>, smem);
-  if (e != cudaSuccess)
-    return e;
-  return allow_smem(dg_stage_kernel<DIM, N, S::NT, S::MINB, MODE_RHS, CT>,
-                    smem);
+  cudaError_t e = allow_smem(single_kernel<DIM, N, CT, MODE_STAGE>, smem);
+  if (e == cudaSuccess)
+    e = allow_smem(single_kernel<DIM, N, CT, MODE_RHS>, smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ[MODE_STAGE], single_kernel<DIM, N, CT, MODE_STAGE>, S::NT, smem);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ[MODE_RHS], single_kernel<DIM, N, CT, MODE_RHS>, S::NT, smem);
+  return e;
 }
 
 template <int DIM, int N, typename CT> KernelSet make_set()
@@ -90,6 +101,7 @@ template <int DIM, int N, typename CT> KernelSet make_set()
   k.energy = dg_energy_kernel<DIM, N>;
   k.NT = S::NT;
   k.smem = stage_smem_bytes<DIM, N, CT>();
+  k.nbuf = nbuf<DIM, N, CT>();
   return k;
 }
 
@@ -261,15 +273,20 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double C,
   // one launch per level; level l's elements after level l-1's
   for (int l = 0; l < d->nlevels; ++l)
   {
-    int grid = d->K;
+    int n = d->K;
     if (d->nlevels > 1)
     {
       v.elist = d->elist + d->level_off[l];
-      grid = d->level_off[l + 1] - d->level_off[l];
+      n = d->level_off[l + 1] - d->level_off[l];
     }
-    if (grid == 0)
+    if (n == 0)
       continue;
-    d->ks.launch(v, sp, d->hops.data(), mode, grid, d->stream);
+    // two element buffers: a persistent grid (every resident CTA slot)
+    // whose CTAs overlap the next element's loads with the current one; one
+    // buffer: one CTA per element, balanced by the block scheduler
+    const int64_t slots = (int64_t)d->ks.occ[mode] * d->sms;
+    const int grid = d->ks.nbuf == 2 && n > slots ? (int)slots : n;
+    d->ks.launch(v, n, sp, d->hops.data(), mode, grid, d->stream);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     CUDA_TRY(cudaGetLastError());
   }
@@ -661,11 +678,17 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
       return fail(BFAM_GPU_ECUDA, "stream: %s", cudaGetErrorString(ce));
     }
     d->own_stream = true;
-    ce = ks.prepare();
+    ce = ks.prepare(d->ks.occ);
+    if (ce == cudaSuccess && (d->ks.occ[0] < 1 || d->ks.occ[1] < 1))
+      ce = cudaErrorInvalidConfiguration;
+    if (ce == cudaSuccess)
+      ce = cudaDeviceGetAttribute(&d->sms, cudaDevAttrMultiProcessorCount,
+                                  d->device);
     if (ce != cudaSuccess)
     {
       release(d);
-      return fail(BFAM_GPU_ECUDA, "smem attribute: %s", cudaGetErrorString(ce));
+      return fail(BFAM_GPU_ECUDA, "stage kernel setup: %s",
+                  cudaGetErrorString(ce));
     }
   }
   d->hops = ops;

@@ -56,84 +56,102 @@ __device__ __forceinline__ int nth_bit(int m, int i)
   return __ffs(m) - 1;
 }
 
-// One element of one stage.  `iter` counts the elements this CTA has done
-// (mbarrier phase parity); the barriers must have been initialised.
-template <int DIM, int N, int NT, int MODE, typename CT>
-__device__ __forceinline__ void stage_element(const DomainView &d,
-                                              const StageParams &sp,
-                                              const DiffOp<N, CT> &dop, int e,
-                                              unsigned iter)
+// Shared-memory layout of one CTA (in doubles, every region 16-byte
+// aligned).  NBUF element buffers (state, dq, face traces / lifted
+// contributions, face flux constants) let the loads of the next element fly
+// while the current one is computed; the mortar scratch, the 1-D operators,
+// the mbarriers (q and dq per buffer) and the precision form's FP32 tile are
+// single.
+template <int DIM, int N, typename CT, int NBUF> struct Tile
 {
   using S = Shape<DIM, N>;
-  constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
-                NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
-                NTF = S::NTF;
-  static_assert(NT >= NF * Nfp, "one face-node work item per thread");
-  // the dynamic shared array itself (not a pointer parameter), so that all
-  // accesses stay in the shared window with 32-bit addressing
-  extern __shared__ __align__(16) double smem[];
-  double *qs = smem;
-  double *R = qs + S::SM_QS;   // dq tile
-  double *pt = R + S::SM_DQ;   // [NF][NFLD][Nfp] plus traces, then lifted
-  double *mj = pt + S::SM_PT;  // [DIM][NJ][Nfp] coarse-side jumps, by fine rank
-  double *fcf = mj + S::SM_MJ; // [NF][4] face flux constants
-  double *sE = fcf + 4 * NF;   // element record
-  CT *sD = reinterpret_cast<CT *>(sE + 8); // differentiation matrix
-  CT *sIb = reinterpret_cast<CT *>(sE + 8 + Nq * Nq); // mortar operators
-  double *sPb = sE + 8 + 2 * Nq * Nq;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sE + 8 + S::SM_IP);
-  // the volume pass's copy of q: q itself in the plain form; in the
-  // precision form FP32 q minus the element's first node per field (the
-  // derivative of a constant is zero), so that rounding is relative to the
-  // variation inside the element
-  constexpr bool NARROW = sizeof(CT) < sizeof(double);
-  CT *qv;
-  if constexpr (NARROW)
-    qv = reinterpret_cast<CT *>(smem + S::SM_TOTAL);
-  else
-    qv = qs;
+  static constexpr int BUF = S::SM_QS + S::SM_DQ + S::SM_PT + 4 * S::NF;
+  static constexpr int OFF_MJ = NBUF * BUF;
+  static constexpr int OFF_OPS = OFF_MJ + S::SM_MJ;
+  static constexpr int OFF_BAR = OFF_OPS + S::SM_IP;
+  static constexpr int OFF_QV = OFF_BAR + 2 * NBUF;
+  static constexpr bool NARROW = sizeof(CT) < sizeof(double);
+  static constexpr int TOTAL = OFF_QV + (NARROW ? S::SM_QF : 0);
+  static constexpr size_t BYTES = (size_t)TOTAL * sizeof(double);
+};
 
+// CTAs per SM that the shape's register budget and NBUF buffers admit
+// (228 KB of shared memory per SM, 1 KB reserved per CTA)
+template <int DIM, int N, typename CT, int NBUF>
+__host__ __device__ constexpr int resident_ctas()
+{
+  constexpr size_t bytes = Tile<DIM, N, CT, NBUF>::BYTES;
+  constexpr int by_smem = bytes > 227 * 1024 ? 0 : (int)(233472 / (bytes + 1024));
+  return Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
+}
+
+// Two buffers (loads of the next element overlap the current one) unless
+// they cost resident CTAs, which hide latency better (e.g. N = 5: three
+// CTAs of 7 warps with one buffer, two with two).
+template <int DIM, int N, typename CT> __host__ __device__ constexpr int nbuf()
+{
+  return resident_ctas<DIM, N, CT, 2>() >= resident_ctas<DIM, N, CT, 1>() &&
+                 resident_ctas<DIM, N, CT, 2>() > 0
+             ? 2
+             : 1;
+}
+
+// Element buffer b of the tile.
+template <int DIM, int N, typename CT, int NBUF> struct TileBuf
+{
+  double *qs, *R, *pt, *fcf;
+  uint64_t *bq, *bdq;
+  __device__ __forceinline__ explicit TileBuf(int b)
+  {
+    using S = Shape<DIM, N>;
+    using T = Tile<DIM, N, CT, NBUF>;
+    extern __shared__ __align__(16) double smem[];
+    qs = smem + b * T::BUF;
+    R = qs + S::SM_QS;
+    pt = R + S::SM_DQ;
+    fcf = pt + S::SM_PT;
+    bq = reinterpret_cast<uint64_t *>(smem + T::OFF_BAR) + 2 * b;
+    bdq = bq + 1;
+  }
+};
+
+// Issue every global read of element e into buffer b: q and (after the first
+// stage) dq by TMA bulk copies completing on the buffer's mbarriers, the
+// neighbours' face traces and the face flux constants by cp.async, as one
+// commit group.
+template <int DIM, int N, int NT, int MODE, typename CT, int NBUF>
+__device__ __forceinline__ void issue_element(const DomainView &d,
+                                              const StageParams &sp, int e,
+                                              int b)
+{
+  using S = Shape<DIM, N>;
+  constexpr int Np = S::Np, Nfp = S::Nfp, NF = S::NF, NFLD = S::NFLD,
+                NTF = S::NTF;
+  const TileBuf<DIM, N, CT, NBUF> tb(b);
+  double *qs = tb.qs, *R = tb.R, *pt = tb.pt, *fcf = tb.fcf;
+  uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
   const int t = threadIdx.x;
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
-  const unsigned par = iter & 1u;
-  // the update is dq = a dq + s rhs; the right-hand-side mode uses a = 0, s = 1
   const bool rd = MODE == MODE_STAGE && !sp.first_stage;
-  const double a = MODE == MODE_STAGE ? sp.A : 0.0;
-  const double s = MODE == MODE_STAGE ? d.dt : 1.0;
-  const ElemData me = d.ed[e];
   const int2 *desc = d.fdesc + (size_t)e * NF;
-
-  int coarse_mask = 0, fine_mask = 0;
-  bool permuted = false; // a glue face whose partner nodes are permuted
-#pragma unroll
-  for (int f = 0; f < NF; ++f)
-  {
-    const int y = desc[f].y;
-    coarse_mask |= ((y & 3) == 2) << f;
-    fine_mask |= ((y & 3) == 1 && ((y >> 8) & 7) != 0) << f;
-    permuted |= (y & 3) == 1 && ((y >> 5) & 7) != 0;
-  }
-  const int ncoarse = __popc(coarse_mask), nfine = __popc(fine_mask);
-
-  // ---------------------------------------------------------- phase 0: issue
   if constexpr (S::TMA)
   {
     if (t == 0)
     {
       fence_proxy_async(); // shared memory of the previous element is free
-      mbar_expect_tx(&bar[0], NFLD * Np * sizeof(double));
+      mbar_expect_tx(bar_q, NFLD * Np * sizeof(double));
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
         bulk_g2s(qs + c * Np, d.qin + c * fs + eoff, Np * sizeof(double),
-                 &bar[0]);
+                 bar_q);
       if (rd)
       {
-        mbar_expect_tx(&bar[1], NFLD * Np * sizeof(double));
+        mbar_expect_tx(bar_dq, NFLD * Np * sizeof(double));
 #pragma unroll
         for (int c = 0; c < NFLD; ++c)
           bulk_g2s(R + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
-                   &bar[1]);
+                   bar_dq);
       }
     }
   }
@@ -173,26 +191,73 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
       cp_async16(fcf + 4 * f + 2, fc + 2);
     }
   }
-  if (t < 4)
-    cp_async16(sE + 2 * t,
-               reinterpret_cast<const double *>(d.ed + e) + 2 * t);
   cp_async_commit(); // own state (non-TMA path), face traces, constants
 
-  // 1-D operators into shared memory (indexed per thread later)
-  for (int w = t; w < Nq * Nq; w += NT)
+}
+
+// Compute element e from buffer b (its loads issued by issue_element; `par`
+// is the buffer's mbarrier phase parity).
+template <int DIM, int N, int NT, int MODE, typename CT, int NBUF>
+__device__ __forceinline__ void compute_element(const DomainView &d,
+                                                const StageParams &sp,
+                                                const DiffOp<N, CT> &dop,
+                                                int e, int b, unsigned par)
+{
+  using S = Shape<DIM, N>;
+  using T = Tile<DIM, N, CT, NBUF>;
+  constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
+                NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
+                NTF = S::NTF;
+  static_assert(NT >= NF * Nfp, "one face-node work item per thread");
+  // the dynamic shared array itself (not a pointer parameter), so that all
+  // accesses stay in the shared window with 32-bit addressing
+  extern __shared__ __align__(16) double smem[];
+  const TileBuf<DIM, N, CT, NBUF> tb(b);
+  double *qs = tb.qs, *R = tb.R, *pt = tb.pt, *fcf = tb.fcf;
+  uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
+  double *mj = smem + T::OFF_MJ; // [DIM][NJ][Nfp] coarse-side jumps, by fine rank
+  const CT *sD = reinterpret_cast<const CT *>(smem + T::OFF_OPS); // D
+  const double *sPb = smem + T::OFF_OPS + 2 * Nq * Nq; // projection
+  // the volume pass's copy of q: q itself in the plain form; in the
+  // precision form FP32 q minus the element's first node per field (the
+  // derivative of a constant is zero), so that rounding is relative to the
+  // variation inside the element
+  constexpr bool NARROW = T::NARROW;
+  CT *qv;
+  if constexpr (NARROW)
+    qv = reinterpret_cast<CT *>(smem + T::OFF_QV);
+  else
+    qv = qs;
+
+  const int t = threadIdx.x;
+  const size_t fs = d.fs;
+  const size_t eoff = (size_t)e * Np;
+  // the update is dq = a dq + s rhs; the right-hand-side mode uses a = 0, s = 1
+  const bool rd = MODE == MODE_STAGE && !sp.first_stage;
+  const double a = MODE == MODE_STAGE ? sp.A : 0.0;
+  const double s = MODE == MODE_STAGE ? d.dt : 1.0;
+  const ElemData me = d.ed[e];
+  const int2 *desc = d.fdesc + (size_t)e * NF;
+
+  int coarse_mask = 0, fine_mask = 0;
+  bool permuted = false; // a glue face whose partner nodes are permuted
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
   {
-    sD[w] = dop.D[w];
-    sIb[w] = dop.Ib[w];
-    sPb[w] = dop.Pb[w];
+    const int y = desc[f].y;
+    coarse_mask |= ((y & 3) == 2) << f;
+    fine_mask |= ((y & 3) == 1 && ((y >> 8) & 7) != 0) << f;
+    permuted |= (y & 3) == 1 && ((y >> 5) & 7) != 0;
   }
+  const int ncoarse = __popc(coarse_mask), nfine = __popc(fine_mask);
 
   // ------------------------------------------------- phase 1: faces, mortars
   if constexpr (S::TMA)
   {
-    if (!mbar_wait(&bar[0], par))
+    if (!mbar_wait(bar_q, par))
       atomicExch(d.err, 1);
   }
-  cp_async_wait<0>();
+  cp_async_wait<NBUF - 1>(); // this element's group (the next one may fly)
   if constexpr (NARROW && !S::TMA)
     __syncthreads(); // other threads' cp.async writes of q
   if constexpr (NARROW)
@@ -356,7 +421,7 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   {
     if constexpr (S::TMA)
     {
-      if (!mbar_wait(&bar[1], par))
+      if (!mbar_wait(bar_dq, par))
         atomicExch(d.err, 2);
     }
   }
@@ -433,64 +498,134 @@ __device__ __forceinline__ void stage_element(const DomainView &d,
   }
 }
 
-__device__ __forceinline__ void stage_barriers_init(int offset)
+
+// The launch's work items: item.view(idx) and item.elem(idx) give item idx's
+// domain view and element.  With one buffer every CTA does one item (the
+// grid covers them all); with two buffers the grid is persistent (items
+// blockIdx.x, blockIdx.x + gridDim.x, ...) and the loads of the next item
+// are issued before the current one is computed.
+template <int DIM, int N, int NT, int MODE, typename CT, int NBUF,
+          typename Item>
+__device__ __forceinline__ void stage_loop(const Item &item, int n,
+                                           const StageParams &sp,
+                                           const DiffOp<N, CT> &dop)
 {
+  using T = Tile<DIM, N, CT, NBUF>;
+  constexpr int Nq = N + 1;
   extern __shared__ __align__(16) double smem[];
   if (threadIdx.x == 0)
   {
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + offset);
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::OFF_BAR);
+    for (int i = 0; i < 2 * NBUF; ++i)
+      mbar_init(&bar[i], 1);
+  }
+  // 1-D operators into shared memory (indexed per thread later)
+  {
+    CT *sD = reinterpret_cast<CT *>(smem + T::OFF_OPS);
+    CT *sIb = reinterpret_cast<CT *>(smem + T::OFF_OPS + Nq * Nq);
+    double *sPb = smem + T::OFF_OPS + 2 * Nq * Nq;
+    for (int w = threadIdx.x; w < Nq * Nq; w += NT)
+    {
+      sD[w] = dop.D[w];
+      sIb[w] = dop.Ib[w];
+      sPb[w] = dop.Pb[w];
+    }
   }
   __syncthreads();
+  int idx = blockIdx.x;
+  if (idx >= n)
+    return;
+  if constexpr (NBUF == 1)
+  {
+    // one element per CTA (the grid covers every item)
+    issue_element<DIM, N, NT, MODE, CT, 1>(item.view(idx), sp, item.elem(idx),
+                                           0);
+    compute_element<DIM, N, NT, MODE, CT, 1>(item.view(idx), sp, dop,
+                                             item.elem(idx), 0, 0);
+    return;
+  }
+  issue_element<DIM, N, NT, MODE, CT, NBUF>(item.view(idx), sp,
+                                            item.elem(idx), 0);
+#pragma unroll 1
+  for (unsigned it = 0; idx < n; ++it)
+  {
+    const int b = (int)(it & 1u);
+    const unsigned par = (it >> 1) & 1u;
+    const int nidx = idx + (int)gridDim.x;
+    if (nidx < n)
+      issue_element<DIM, N, NT, MODE, CT, NBUF>(item.view(nidx), sp,
+                                                item.elem(nidx), b ^ 1);
+    else
+      cp_async_commit(); // keep one group per iteration
+    compute_element<DIM, N, NT, MODE, CT, NBUF>(item.view(idx), sp, dop,
+                                                item.elem(idx), b, par);
+    __syncthreads(); // buffer b is free
+    idx = nidx;
+  }
 }
 
-template <int DIM, int N> __host__ __device__ constexpr int bar_offset()
+// one domain: item idx is element idx, or the idx-th of an element list
+struct SingleItems
 {
-  using S = Shape<DIM, N>;
-  return S::SM_QS + S::SM_DQ + S::SM_PT + S::SM_MJ + S::SM_FC + S::SM_IP;
-}
+  const DomainView &d;
+  __device__ __forceinline__ const DomainView &view(int) const { return d; }
+  __device__ __forceinline__ int elem(int idx) const
+  {
+    return d.elist ? d.elist[idx] : idx;
+  }
+};
 
-// dynamic shared memory of one CTA of the stage kernel
-template <int DIM, int N, typename CT>
-__host__ __device__ constexpr size_t stage_smem_bytes()
+// many domains: item idx is work[idx] = (domain, element)
+struct BatchItems
 {
-  using S = Shape<DIM, N>;
-  return (S::SM_TOTAL + (sizeof(CT) < sizeof(double) ? S::SM_QF : 0)) *
-         sizeof(double);
-}
+  const DomainView *__restrict__ views;
+  const int2 *__restrict__ work;
+  __device__ __forceinline__ const DomainView &view(int idx) const
+  {
+    return views[work[idx].x];
+  }
+  __device__ __forceinline__ int elem(int idx) const { return work[idx].y; }
+};
 
-// One domain, one element per CTA: element blockIdx.x, or the
-// blockIdx.x-th of the launch's element list (meshes with hanging faces
-// launch their elements by level).
-template <int DIM, int N, int NT, int MINB, int MODE, typename CT>
+// One domain: item idx is element idx, or the idx-th of the launch's
+// element list (meshes with hanging faces launch their elements by level).
+template <int DIM, int N, int NT, int MINB, int MODE, typename CT, int NBUF>
 __global__ void __launch_bounds__(NT, MINB)
-    dg_stage_kernel(DomainView d, StageParams sp,
+    dg_stage_kernel(DomainView d, int n, StageParams sp,
                     const __grid_constant__ DiffOp<N, CT> dop)
 {
-  stage_barriers_init(bar_offset<DIM, N>());
-  const int e = d.elist ? d.elist[blockIdx.x] : (int)blockIdx.x;
-  stage_element<DIM, N, NT, MODE, CT>(d, sp, dop, e, 0);
+  stage_loop<DIM, N, NT, MODE, CT, NBUF>(SingleItems{d}, n, sp, dop);
 }
 
-// Many domains of the same order in one persistent launch: CTAs stride over
-// a flat work list of (domain, element) pairs, each domain with its own
-// arrays and time step.
-template <int DIM, int N, int NT, int MINB, int MODE, typename CT>
+// Many domains of the same order: item idx is work[idx] = (domain, element),
+// each domain with its own arrays and time step.
+template <int DIM, int N, int NT, int MINB, int MODE, typename CT, int NBUF>
 __global__ void __launch_bounds__(NT, MINB)
     dg_stage_batch_kernel(const DomainView *__restrict__ views,
                           const int2 *__restrict__ work, int nwork,
                           StageParams sp,
                           const __grid_constant__ DiffOp<N, CT> dop)
 {
-  stage_barriers_init(bar_offset<DIM, N>());
-  unsigned iter = 0;
-  for (int i = blockIdx.x; i < nwork; i += gridDim.x, ++iter)
-  {
-    const int2 w = work[i];
-    stage_element<DIM, N, NT, MODE, CT>(views[w.x], sp, dop, w.y, iter);
-    __syncthreads(); // shared memory is reused by the next element
-  }
+  stage_loop<DIM, N, NT, MODE, CT, NBUF>(BatchItems{views, work}, nwork, sp,
+                                         dop);
+}
+
+// dynamic shared memory of one CTA of the stage kernels
+template <int DIM, int N, typename CT>
+__host__ __device__ constexpr size_t stage_smem_bytes()
+{
+  return Tile<DIM, N, CT, nbuf<DIM, N, CT>()>::BYTES;
+}
+
+// resident CTAs per SM the register budget is sized for: the shape's choice,
+// capped by what the shared memory allows (228 KB per SM, 1 KB reserved per
+// CTA)
+template <int DIM, int N, typename CT>
+__host__ __device__ constexpr int stage_min_ctas()
+{
+  constexpr int by_smem = (int)(233472 / (stage_smem_bytes<DIM, N, CT>() + 1024));
+  constexpr int m = Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
+  return m < 1 ? 1 : m;
 }
 
 } // namespace bfam_b200

@@ -29,10 +29,10 @@ extern std::atomic<uint64_t> g_launches;
   } while (0)
 
 // per-order launchers (the kernels' parameter lists depend on the order)
-typedef void (*stage_launch_fn)(const DomainView &, const StageParams &,
-                                const double *D, int mode, int grid,
-                                cudaStream_t);
-typedef cudaError_t (*prepare_fn)();
+typedef void (*stage_launch_fn)(const DomainView &, int n,
+                                const StageParams &, const double *D,
+                                int mode, int grid, cudaStream_t);
+typedef cudaError_t (*prepare_fn)(int *occ);
 typedef void (*energy_fn)(const double *, size_t, const ElemData *,
                           const double *, double *);
 
@@ -43,6 +43,8 @@ struct KernelSet
   energy_fn energy = nullptr;
   int NT = 0;
   size_t smem = 0;
+  int occ[2] = {0, 0}; // resident CTAs per SM of the stage and rhs kernels
+  int nbuf = 1;        // element buffers per CTA
 };
 
 // the kernels of one (dim, order, precision)
@@ -71,7 +73,7 @@ struct bfam_gpu_domain
 {
   int dim = 0, N = 0, Nq = 0, Np = 0, Nfp = 0, NF = 0, NFLD = 0;
   int32_t K = 0, Kg = 0;
-  int device = 0;
+  int device = 0, sms = 0;
   int flux = 0, precision = 0;
   size_t fs = 0;
   bfam_b200::host::KernelSet ks;
