@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg1",
                     choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--periods", type=float, default=1.0,
+                    help="cfg2: periods of the analytic plane wave")
     ap.add_argument("--rates", default="10,50,200,500",
                     help="cfg4: Poisson arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate")
@@ -393,6 +395,105 @@ def run_batched(args):
     return 0
 
 
+def _field_errors(a, b):
+    """per-field relative L2 of a against b; a (nearly) zero field is
+    measured against the largest field's norm"""
+    num = np.sqrt(((a - b) ** 2).sum(axis=1))
+    den = np.sqrt((b ** 2).sum(axis=1))
+    den = np.where(den > 1e-8 * den.max(), den, den.max())
+    return [float(x) for x in num / den]
+
+
+def run_precision(args):
+    """cfg2: the precision form (FP32 right-hand side, FP64 state) at N=7 on
+    cfg1's mesh: throughput against the plain FP64 form on the heterogeneous
+    material, the error against FP64 after the timed steps, and one period
+    of the analytic P plane wave (homogeneous material) in both forms."""
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    import bfam_b200 as bf
+    from bfam_b200 import configs
+
+    W = max(3, args.warmup)
+    p = configs.cfg2(n=args.n)
+    out = {}
+    states = {}
+    n0 = bf.launch_count()
+    with ClockSampler(local) as clk:
+        for name, prec in (("fp32", bf.PRECISION_FP32), ("fp64", bf.PRECISION_FP64)):
+            dom = bf.GpuDomain(p.mesh, p.rho, p.lam, p.mu, precision=prec, device=local)
+            stream = torch.cuda.Stream(device=local)
+            dom.set_stream(stream.cuda_stream)
+            dom.set_fields(p.q0)
+            ts = bf.LSRK(dom)
+            ts.step(p.dt, W, use_graph=True)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ts.step(p.dt, args.steps, use_graph=True)
+            e1.record(stream)
+            e1.synchronize()
+            t = e0.elapsed_time(e1) / 1e3
+            out[name] = p.ndof * 5 * args.steps / t
+            states[name] = dom.get_fields()
+            ts.free()
+            dom.free()
+    launches = bf.launch_count() - n0
+    err_het = _field_errors(states["fp32"], states["fp64"])
+    del states
+    # analytic plane wave over `periods` periods on the same mesh
+    pw = configs.plane_wave_3d(7, args.n, periods=args.periods)
+    r = bf.lgl_operators(7)[0]
+    qe = pw.mesh.plane_wave(r, pw.meta["k"], 1.0, 1.0, 2.0, 1.0, pw.meta["T"])
+    res = {}
+    for name, prec in (("fp32", bf.PRECISION_FP32), ("fp64", bf.PRECISION_FP64)):
+        dom = bf.GpuDomain(pw.mesh, pw.rho, pw.lam, pw.mu, precision=prec, device=local)
+        dom.set_fields(pw.q0)
+        bf.LSRK(dom).step(pw.dt, pw.nsteps, use_graph=True)
+        res[name] = dom.get_fields()
+        dom.free()
+    names = list(bf.FIELDS_3D)
+    scale = np.sqrt((qe ** 2).sum())
+    plane = {
+        "steps": pw.nsteps, "dt": pw.dt, "T": pw.meta["T"],
+        "rel_l2_vs_analytic": {k: float(np.sqrt(((res[k] - qe) ** 2).sum()) / scale)
+                               for k in res},
+        "rel_l2_fp32_vs_fp64_per_field": dict(zip(names, _field_errors(res["fp32"], res["fp64"]))),
+        "rel_l2_vs_analytic_per_field": {
+            k: dict(zip(names, [float(np.sqrt(((res[k][f] - qe[f]) ** 2).sum()) / scale)
+                                for f in range(9)])) for k in res},
+        "note": "per-field errors against the analytic solution are relative to the "
+                "whole state's norm (vy, vz and the shear stresses are zero)",
+    }
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        ach = p.ndof * ALG_BYTES_PER_DOF_UPDATE[5] * 5 * out["fp32"] / (p.ndof * 5) / 1e9
+        line = {
+            "metric": "DOF-updates/s", "value": out["fp32"], "unit": "DOF-updates/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": W,
+            "ms_per_step": p.ndof * 5 / out["fp32"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 rhs / f64 state",
+            "data": "synthetic",
+            "config": dict(workload_desc(p), parallelism=f"replicas{ws}", cuda_graph=True),
+            "precision_form": {
+                "fp32_value": out["fp32"], "fp64_value": out["fp64"],
+                "speedup_vs_plain_fp64": out["fp32"] / out["fp64"],
+                "heterogeneous_rel_l2_fp32_vs_fp64_per_field": dict(zip(names, err_het)),
+                "heterogeneous_steps": W + args.steps,
+                "plane_wave": plane,
+            },
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_source": f"of {peak_kind}",
+                         "traffic": None,
+                         "kernel": "dg_stage_kernel N=7 precision form"},
+            "cpu_baseline": None, "e2e": None,
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_serving(args):
     """cfg4: Poisson streams of point-source requests through the
     continuous-batching server, one run per arrival rate."""
@@ -478,6 +579,8 @@ def main():
         return run_reference(args)
     if args.config == "cfg3":
         return run_batched(args)
+    if args.config == "cfg2":
+        return run_precision(args)
     if args.config == "cfg4":
         return run_serving(args)
     import torch
