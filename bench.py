@@ -160,7 +160,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def dist_init():
+def dist_init(backend=None):
+    """One process per GPU (torchrun's environment); NCCL on GPUs, gloo
+    without.  The replicas share no data: the group only times them."""
     import torch
     import torch.distributed as dist
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -168,10 +170,32 @@ def dist_init():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1 and not dist.is_initialized():
         import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        kw = {}
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            kw["device_id"] = torch.device("cuda", local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600), **kw)
     return ws, rank, local
+
+
+def max_over_ranks(x: float, local: int = 0) -> float:
+    """Max of a per-rank value (a device-timed interval) over the process
+    group; the value itself on one process."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return x
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank: float, t_max: float, ws: int) -> float:
+    """Whole-job throughput of ws independent replicas: every rank's units
+    over the slowest rank's time."""
+    return units_per_rank * ws / t_max
 
 
 def cpu_baseline_sample(p, budget_s=12.0):
@@ -279,12 +303,8 @@ def run_batched(args):
     launches = bf.launch_count() - n0
     batch.sync()
     t_local = ev0.elapsed_time(ev1) / 1e3
-    t_max = t_local
-    if ws > 1:
-        t = torch.tensor([t_local], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = total * 5 * args.steps * ws / t_max
+    t_max = max_over_ranks(t_local, local)
+    value = replica_value(total * 5 * args.steps, t_max, ws)
     peak, peak_kind = measured_peak()
     achieved = total * 5 * ALG_BYTES_PER_DOF_UPDATE[5] * args.steps / t_local / 1e9
 
@@ -620,17 +640,13 @@ def main():
     dom.sync()
     ms = ev0.elapsed_time(ev1)
     t_local = ms / 1e3
+    t_max = max_over_ranks(t_local, local)
     if ws > 1:
-        t = torch.tensor([t_local], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
         torch.cuda.synchronize()
-        t_max = float(t.item())
-    else:
-        t_max = t_local
     ns = 5
     dof_updates = p.ndof * ns * args.steps
-    value = dof_updates * ws / t_max
+    value = replica_value(dof_updates, t_max, ws)
 
     # roofline of the dominant (only) kernel, the fused stage kernel, per
     # LSRK stage: one launch per refinement level (level 0, then the
@@ -669,10 +685,7 @@ def main():
         e1.record(stream)
         e1.synchronize()
         el = e0.elapsed_time(e1) / 1e3
-        if ws > 1:
-            t = torch.tensor([el], device=f"cuda:{local}", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(el, local)
         nbytes = host_np.nbytes
         e2e = {"value": p.ndof * ns * p.nsteps * ws / el, "unit": "DOF-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
