@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate")
     ap.add_argument("--chunk", type=int, default=25, help="cfg4: steps per batch chunk")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
-                    help="arithmetic of the right-hand side (default: fp64; cfg3: fp32)")
+                    help="arithmetic of the right-hand side (default: fp64; cfg3, cfg4: "
+                         "fp32); with cfg2 it times that one form only, as cfg1 does")
     ap.add_argument("--instances", type=int, default=256, help="cfg3: number of instances")
     ap.add_argument("--sample", type=int, default=24,
                     help="cfg3: instances also solved alone in FP64 (plain form) for "
@@ -605,7 +606,7 @@ def main():
         return run_reference(args)
     if args.config == "cfg3":
         return run_batched(args)
-    if args.config == "cfg2":
+    if args.config == "cfg2" and args.precision is None:
         return run_precision(args)
     if args.config == "cfg4":
         return run_serving(args)

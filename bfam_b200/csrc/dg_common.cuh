@@ -124,13 +124,18 @@ template <int DIM, int N> struct Shape
   static constexpr int ROWS = DIM == 3 ? Nq : 1; // rows of a face
   static constexpr int NL = Np / Nq;              // lines per direction
   static constexpr int NDF = DIM == 3 ? 6 : 4; // fields differentiated per axis
-  static constexpr int work = (Np > NF * Nfp ? Np : NF * Nfp);
+  // one thread per node, or per face node where those are fewer (3D N=7:
+  // 384 face nodes, 512 nodes in two passes, so that two CTAs fit an SM)
+  static constexpr int work =
+      (DIM == 3 && N == 7) ? NF * Nfp : (Np > NF * Nfp ? Np : NF * Nfp);
   static constexpr int NT = ((work + 31) / 32) * 32 > 1024
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
   // CTAs per SM the register allocation is sized for (about 96 registers)
   static constexpr int MINB_RAW = 65536 / (NT * 96);
-  static constexpr int MINB = MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW);
+  static constexpr int MINB = (DIM == 3 && N == 7)
+                                  ? 2
+                                  : (MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW));
   static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
   // shared memory regions in doubles (all even, so 16-byte aligned)
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q
@@ -182,6 +187,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::"
                "bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// bulk prefetch of a 16-byte aligned global range into L2 (no completion)
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes)
+{
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src),
+               "r"(bytes)
                : "memory");
 }
 

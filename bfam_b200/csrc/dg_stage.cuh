@@ -62,10 +62,13 @@ __device__ __forceinline__ int nth_bit(int m, int i)
 // while the current one is computed; the mortar scratch, the 1-D operators,
 // the mbarriers (q and dq per buffer) and the precision form's FP32 tile are
 // single.
-template <int DIM, int N, typename CT, int NBUF> struct Tile
+template <int DIM, int N, typename CT, int NBUF, bool DQS = true> struct Tile
 {
   using S = Shape<DIM, N>;
-  static constexpr int BUF = S::SM_QS + S::SM_DQ + S::SM_PT + 4 * S::NF;
+  // DQS: the element's dq rows are staged in shared memory (TMA); otherwise
+  // they are prefetched into L2 and read from global memory by the update
+  static constexpr int BUF =
+      S::SM_QS + (DQS ? S::SM_DQ : 0) + S::SM_PT + 4 * S::NF;
   static constexpr int OFF_MJ = NBUF * BUF;
   static constexpr int OFF_OPS = OFF_MJ + S::SM_MJ;
   static constexpr int OFF_BAR = OFF_OPS + S::SM_IP;
@@ -77,12 +80,21 @@ template <int DIM, int N, typename CT, int NBUF> struct Tile
 
 // CTAs per SM that the shape's register budget and NBUF buffers admit
 // (228 KB of shared memory per SM, 1 KB reserved per CTA)
-template <int DIM, int N, typename CT, int NBUF>
+template <int DIM, int N, typename CT, int NBUF, bool DQS = true>
 __host__ __device__ constexpr int resident_ctas()
 {
-  constexpr size_t bytes = Tile<DIM, N, CT, NBUF>::BYTES;
+  constexpr size_t bytes = Tile<DIM, N, CT, NBUF, DQS>::BYTES;
   constexpr int by_smem = bytes > 227 * 1024 ? 0 : (int)(233472 / (bytes + 1024));
   return Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
+}
+
+// dq staged in shared memory unless leaving it out (prefetching it into L2
+// and reading it in the update) admits more resident CTAs (3D N=7 in the
+// precision form: two CTAs instead of one)
+template <int DIM, int N, typename CT> __host__ __device__ constexpr bool stage_dqs()
+{
+  return resident_ctas<DIM, N, CT, 1, true>() >=
+         resident_ctas<DIM, N, CT, 1, false>();
 }
 
 // Two buffers (loads of the next element overlap the current one) unless
@@ -90,8 +102,10 @@ __host__ __device__ constexpr int resident_ctas()
 // CTAs of 7 warps with one buffer, two with two).
 template <int DIM, int N, typename CT> __host__ __device__ constexpr int nbuf()
 {
-  return resident_ctas<DIM, N, CT, 2>() >= resident_ctas<DIM, N, CT, 1>() &&
-                 resident_ctas<DIM, N, CT, 2>() > 0
+  constexpr bool DQS = stage_dqs<DIM, N, CT>();
+  return resident_ctas<DIM, N, CT, 2, DQS>() >=
+                     resident_ctas<DIM, N, CT, 1, DQS>() &&
+                 resident_ctas<DIM, N, CT, 2, DQS>() > 0
              ? 2
              : 1;
 }
@@ -104,11 +118,12 @@ template <int DIM, int N, typename CT, int NBUF> struct TileBuf
   __device__ __forceinline__ explicit TileBuf(int b)
   {
     using S = Shape<DIM, N>;
-    using T = Tile<DIM, N, CT, NBUF>;
+    constexpr bool DQS = stage_dqs<DIM, N, CT>();
+    using T = Tile<DIM, N, CT, NBUF, DQS>;
     extern __shared__ __align__(16) double smem[];
     qs = smem + b * T::BUF;
     R = qs + S::SM_QS;
-    pt = R + S::SM_DQ;
+    pt = R + (DQS ? S::SM_DQ : 0);
     fcf = pt + S::SM_PT;
     bq = reinterpret_cast<uint64_t *>(smem + T::OFF_BAR) + 2 * b;
     bdq = bq + 1;
@@ -147,11 +162,20 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
                  bar_q);
       if (rd)
       {
-        mbar_expect_tx(bar_dq, NFLD * Np * sizeof(double));
+        if constexpr (stage_dqs<DIM, N, CT>())
+        {
+          mbar_expect_tx(bar_dq, NFLD * Np * sizeof(double));
 #pragma unroll
-        for (int c = 0; c < NFLD; ++c)
-          bulk_g2s(R + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
-                   bar_dq);
+          for (int c = 0; c < NFLD; ++c)
+            bulk_g2s(R + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
+                     bar_dq);
+        }
+        else
+        {
+#pragma unroll
+          for (int c = 0; c < NFLD; ++c)
+            bulk_prefetch_l2(d.dq + c * fs + eoff, Np * sizeof(double));
+        }
       }
     }
   }
@@ -160,7 +184,7 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
     for (int w = t; w < NFLD * Np; w += NT)
     {
       cp_async8(qs + w, d.qin + (w / Np) * fs + eoff + (w % Np));
-      if (rd)
+      if (stage_dqs<DIM, N, CT>() && rd)
         cp_async8(R + w, d.dq + (w / Np) * fs + eoff + (w % Np));
     }
   }
@@ -204,7 +228,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
                                                 int e, int b, unsigned par)
 {
   using S = Shape<DIM, N>;
-  using T = Tile<DIM, N, CT, NBUF>;
+  using T = Tile<DIM, N, CT, NBUF, stage_dqs<DIM, N, CT>()>;
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
                 NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
                 NTF = S::NTF;
@@ -417,7 +441,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   __syncthreads();
 
   // ------------------------ phase 2: volume, face contributions and update
-  if (MODE == MODE_STAGE && rd)
+  constexpr bool DQS = stage_dqs<DIM, N, CT>();
+  if (MODE == MODE_STAGE && rd && DQS)
   {
     if constexpr (S::TMA)
     {
@@ -480,7 +505,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       {
 #pragma unroll
         for (int c = 0; c < NFLD; ++c)
-          acc[c] += a * R[c * Np + n];
+          acc[c] += a * (DQS ? R[c * Np + n] : d.dq[c * fs + eoff + n]);
       }
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
@@ -510,7 +535,7 @@ __device__ __forceinline__ void stage_loop(const Item &item, int n,
                                            const StageParams &sp,
                                            const DiffOp<N, CT> &dop)
 {
-  using T = Tile<DIM, N, CT, NBUF>;
+  using T = Tile<DIM, N, CT, NBUF, stage_dqs<DIM, N, CT>()>;
   constexpr int Nq = N + 1;
   extern __shared__ __align__(16) double smem[];
   if (threadIdx.x == 0)
@@ -614,7 +639,7 @@ __global__ void __launch_bounds__(NT, MINB)
 template <int DIM, int N, typename CT>
 __host__ __device__ constexpr size_t stage_smem_bytes()
 {
-  return Tile<DIM, N, CT, nbuf<DIM, N, CT>()>::BYTES;
+  return Tile<DIM, N, CT, nbuf<DIM, N, CT>(), stage_dqs<DIM, N, CT>()>::BYTES;
 }
 
 // resident CTAs per SM the register budget is sized for: the shape's choice,
