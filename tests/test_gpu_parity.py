@@ -148,17 +148,26 @@ def test_memory_budget_is_enforced():
 @pytest.mark.slow
 def test_cfg1_full_size_rhs_parity_and_energy():
     """Full config-1 mesh (32^3, p=0.3, N=5): one RHS against the oracle,
-    then a few steps with decreasing energy."""
+    then K steps against the oracle (per field) with decreasing energy.
+    At t = 0 the pulse has v = 0 and S = -p I, so the stress right-hand side
+    is nonzero only where the traces of p differ across hanging faces: a
+    field ~1e-6 of the state made of trace differences, which the per-field
+    measure would compare against its own cancellation-sized norm; the
+    right-hand side is therefore measured against the largest field, and the
+    per-field bar is applied to the state after the steps."""
     p = configs.cfg1()
+    o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
     dom = bf.GpuDomain(p.mesh, p.rho, p.lam, p.mu)
     dom.set_fields(p.q0)
     got = dom.rhs()
-    ref = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu).rhs(p.q0)
-    # fields that are zero at t=0 have zero rhs in the interior; measure all
-    # against the largest field
-    assert relerr(got, ref).max() < TOL
+    ref = o.rhs(p.q0)
+    num = np.sqrt(((got - ref) ** 2).sum(axis=1))
+    assert (num / np.sqrt((ref ** 2).sum(axis=1)).max()).max() < TOL
     del got, ref
     E0 = dom.energy()
-    bf.LSRK(dom).step(p.dt, 4, use_graph=True)
+    bf.LSRK(dom).step(p.dt, 3, use_graph=True)
     E1 = dom.energy()
     assert np.isfinite(E1) and E1 < E0
+    q = dom.get_fields()
+    qr = o.lsrk(p.q0, p.dt, 3)
+    assert relerr(q, qr).max() < TOL
