@@ -396,6 +396,13 @@ class GpuDomain:
     def device_bytes(self) -> int:
         return int(lib().bfam_gpu_domain_device_bytes(self._h))
 
+    def write_vtu(self, path, time: float | None = None, binary: bool = True):
+        """download the fields and write them as a .vtu file (bfam_b200.vtk)"""
+        from .vtk import write_vtu
+        if self.mesh is None:
+            raise ValueError("the domain no longer holds its mesh")
+        return write_vtu(path, self.mesh, self.get_fields(), time=time, binary=binary)
+
     def launch_levels(self) -> int:
         """launches per LSRK stage (one per refinement level)"""
         return int(lib().bfam_gpu_domain_launch_levels(self._h))
