@@ -20,6 +20,7 @@ FIELDS_2D = ("vx", "vy", "sxx", "syy", "sxy")
 FIELDS_3D = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
 
 FLUX_UPWIND, FLUX_CENTRAL = 0, 1
+BC_FREE_SURFACE, BC_ABSORBING = 0, 1
 # status codes of the C-ABI
 (BFAM_GPU_EINVAL, BFAM_GPU_ENOMEM, BFAM_GPU_ECUDA, BFAM_GPU_ETIMEOUT,
  BFAM_GPU_EUNSUPPORTED) = (-1, -2, -3, -4, -5)
@@ -68,7 +69,8 @@ class MeshStruct(C.Structure):
                 ("EToE", i32p), ("EToF", i8p), ("vmapM", i32p), ("vmapP", i32p),
                 ("Kg", C.c_int32), ("EToEm", i32p), ("EToFm", i8p), ("EToHm", i8p),
                 ("EToEp", i32p), ("EToHp", i8p), ("EToOp", i8p),
-                ("num_refined", C.c_int32)]
+                ("num_refined", C.c_int32),
+                ("Kb", C.c_int32), ("EToEb", i32p), ("EToFb", i8p)]
 
 
 class VolumeDesc(C.Structure):
@@ -81,6 +83,10 @@ class GlueDesc(C.Structure):
     _fields_ = [("K", C.c_int32), ("EToEp", i32p), ("EToHp", i8p), ("EToOp", i8p),
                 ("EToEm", i32p), ("EToFm", i8p), ("EToHm", i8p),
                 ("interpolation", dp * 3), ("projection", dp * 3)]
+
+
+class BoundaryDesc(C.Structure):
+    _fields_ = [("K", C.c_int32), ("EToE", i32p), ("EToF", i8p), ("type", i8p)]
 
 
 class SourceDesc(C.Structure):
@@ -113,6 +119,9 @@ def _declare(L: C.CDLL) -> None:
         "bfam_b200_pcg32_bounded": (C.c_uint32, [vp, C.c_uint32]),
         "bfam_b200_pcg32_uniform": (C.c_double, [vp]),
         "bfam_gpu_domain_create": (C.c_int, [P(VolumeDesc), P(GlueDesc), P(Options), P(vp)]),
+        "bfam_gpu_domain_create_with_boundary": (C.c_int, [P(VolumeDesc), P(GlueDesc),
+                                                           P(BoundaryDesc), P(Options),
+                                                           P(vp)]),
         "bfam_gpu_domain_free": (C.c_int, [vp]),
         "bfam_gpu_domain_num_fields": (C.c_int, [vp]),
         "bfam_gpu_domain_field_length": (C.c_size_t, [vp]),
@@ -230,7 +239,7 @@ class Mesh:
     """Brick mesh in bfam's data model (see bfam_b200_brick_mesh_new)."""
 
     def __init__(self, dim: int, N: int, n, L=(1.0, 1.0, 1.0), refine_prob: float = 0.0,
-                 seed: int = 0, refine_flags=None):
+                 seed: int = 0, refine_flags=None, periodic=(True, True, True)):
         spec = BrickSpec()
         spec.dim, spec.N = dim, N
         nn = list(n) + [1] * (3 - len(n))
@@ -238,7 +247,7 @@ class Mesh:
         for a in range(3):
             spec.n[a] = int(nn[a])
             spec.L[a] = float(LL[a])
-            spec.periodic[a] = 1
+            spec.periodic[a] = 1 if (a >= dim or periodic[a]) else 0
         spec.refine_prob = float(refine_prob)
         spec.seed = int(seed)
         self._flags = None
@@ -254,6 +263,7 @@ class Mesh:
         self.dim, self.N, self.Nq, self.Np = m.dim, m.N, m.Nq, m.Np
         self.Nfp, self.Nfaces, self.K, self.Kg = m.Nfp, m.Nfaces, m.K, m.Kg
         self.nbase = tuple(nn[:3])
+        self.periodic = tuple(bool(spec.periodic[a]) for a in range(3))
         self.L = tuple(LL[:3])
         self.num_refined = m.num_refined
         K, NF, Nfp, Kg = self.K, self.Nfaces, self.Nfp, self.Kg
@@ -274,6 +284,10 @@ class Mesh:
         self.EToEp = arr(m.EToEp, Kg, np.int32)
         self.EToHp = arr(m.EToHp, Kg, np.int8)
         self.EToOp = arr(m.EToOp, Kg, np.int8)
+        # boundary faces of non-periodic axes (element, face)
+        self.Kb = m.Kb
+        self.EToEb = arr(m.EToEb, m.Kb, np.int32)
+        self.EToFb = arr(m.EToFb, m.Kb, np.int8)
 
     def __del__(self):
         try:
@@ -334,7 +348,9 @@ class GpuDomain:
 
     def __init__(self, mesh: Mesh, rho, lam, mu, flux: int = FLUX_UPWIND,
                  precision: int = PRECISION_FP64, mem_budget_bytes: int = 0,
-                 device: int = 0):
+                 device: int = 0, bc=BC_FREE_SURFACE):
+        """bc: the condition on the boundary faces of a non-periodic mesh,
+        one value for every side or one per side (-x, +x, -y, +y, -z, +z)"""
         L = lib()
         self.mesh = mesh
         N = mesh.N
@@ -372,8 +388,22 @@ class GpuDomain:
         opt.flux, opt.precision = flux, precision
         opt.mem_budget_bytes, opt.device = mem_budget_bytes, device
         h = C.c_void_p()
-        _check(L.bfam_gpu_domain_create(C.byref(vol), C.byref(glue), C.byref(opt),
-                                        C.byref(h)))
+        if getattr(mesh, "Kb", 0):
+            sides = np.broadcast_to(np.asarray(bc, dtype=np.int8), (2 * mesh.dim,))
+            btype = np.ascontiguousarray(sides[mesh.EToFb], dtype=np.int8)
+            self._keep += [btype]
+            bnd = BoundaryDesc()
+            bnd.K = mesh.Kb
+            bnd.EToE = mesh.EToEb.ctypes.data_as(i32p)
+            bnd.EToF = mesh.EToFb.ctypes.data_as(i8p)
+            bnd.type = btype.ctypes.data_as(i8p)
+            self.bc = tuple(int(x) for x in sides)
+            _check(L.bfam_gpu_domain_create_with_boundary(
+                C.byref(vol), C.byref(glue), C.byref(bnd), C.byref(opt), C.byref(h)))
+        else:
+            self.bc = None
+            _check(L.bfam_gpu_domain_create(C.byref(vol), C.byref(glue), C.byref(opt),
+                                            C.byref(h)))
         self._h = h
         self.nfields = L.bfam_gpu_domain_num_fields(h)
         self.field_length = L.bfam_gpu_domain_field_length(h)

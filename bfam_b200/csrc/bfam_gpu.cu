@@ -315,6 +315,15 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
                            const bfam_gpu_options_t *opts,
                            bfam_gpu_domain_t **out)
 {
+  return bfam_gpu_domain_create_with_boundary(vol, glue, nullptr, opts, out);
+}
+
+int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
+                                         const bfam_gpu_glue_t *glue,
+                                         const bfam_gpu_boundary_t *bnd,
+                                         const bfam_gpu_options_t *opts,
+                                         bfam_gpu_domain_t **out)
+{
   if (!out)
     return fail(BFAM_GPU_EINVAL, "out is NULL");
   *out = nullptr;
@@ -454,11 +463,38 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
     nbr[(size_t)e * NF + f] = -1 - g;
     g += cnt;
   }
+  // ---- boundary faces: self-mapped and not in the glue grid
+  constexpr int32_t BOUNDARY = INT32_MIN + 1;
+  std::vector<int8_t> bctype(nbr.size(), -1);
+  if (bnd && bnd->K > 0)
+  {
+    if (!bnd->EToE || !bnd->EToF || !bnd->type)
+      return fail(BFAM_GPU_EINVAL, "a required boundary array is NULL");
+    for (int32_t b = 0; b < bnd->K; ++b)
+    {
+      const int32_t e = bnd->EToE[b];
+      const int f = bnd->EToF[b];
+      const int ty = bnd->type[b];
+      if (e < 0 || e >= K || f < 0 || f >= NF)
+        return fail(BFAM_GPU_EINVAL, "boundary face %d has bad (E, F) = (%d, %d)",
+                    b, e, f);
+      if (ty != BFAM_GPU_BC_FREE_SURFACE && ty != BFAM_GPU_BC_ABSORBING)
+        return fail(BFAM_GPU_EINVAL, "boundary face %d has unknown type %d", b,
+                    ty);
+      if (nbr[(size_t)e * NF + f] != INT32_MIN)
+        return fail(BFAM_GPU_EINVAL,
+                    "boundary face %d (element %d face %d) has a neighbour, a "
+                    "glue element or a second boundary entry",
+                    b, e, f);
+      nbr[(size_t)e * NF + f] = BOUNDARY;
+      bctype[(size_t)e * NF + f] = (int8_t)ty;
+    }
+  }
   for (size_t i = 0; i < nbr.size(); ++i)
     if (nbr[i] == INT32_MIN)
       return fail(BFAM_GPU_EINVAL,
                   "element %zu face %zu maps to itself but has no glue "
-                  "element",
+                  "element or boundary entry",
                   i / NF, i % NF);
 
   // ---- mortar buffer slots: one per coarse-side glue element (piece), in
@@ -479,6 +515,11 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
     {
       const int code = nbrf[i];
       fdesc[i] = make_int2(nb, 0 | ((code % NF) << 2) | ((code / NF) << 5));
+      continue;
+    }
+    if (nb == BOUNDARY)
+    {
+      fdesc[i] = make_int2((int32_t)(i / NF), 3 | (bctype[i] << 2));
       continue;
     }
     const int32_t g0 = -1 - nb;
@@ -629,7 +670,7 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
   };
   std::vector<double4> fcE((size_t)K * NF, make_double4(0, 0, 0, 0));
   for (size_t i = 0; i < fcE.size(); ++i)
-    if ((fdesc[i].y & 3) != 2)
+    if ((fdesc[i].y & 3) != 2) // boundary faces: the ghost has my material
       fcE[i] = fconst((int32_t)(i / NF), fdesc[i].x);
 
   // ---- device

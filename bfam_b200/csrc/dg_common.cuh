@@ -22,6 +22,8 @@ struct ElemData
 //   1 glue, whole face:  a = partner element (same size or coarse),
 //                        b>>2 & 7 = partner face, b>>5 & 7 = glue orientation,
 //                        b>>8 & 7 = partner's hanging piece (0: same size)
+//   3 boundary:          a = the element, b>>2 & 3 = condition
+//                        (0 free surface, 1 absorbing)
 //   2 glue, coarse side: a = mortar buffer slot of the face's first piece
 //                        (the pieces' slots are consecutive, in glue order)
 // A fine face (kind 1 with a hanging piece) writes its projected coarse-side

@@ -21,11 +21,12 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT)
   const double *w = ops + 7 * Nq * Nq;
   const ElemData me = ed[e];
   double val = 0;
-  if (t < Np)
+  // NT may be below Np (N = 7 in 3D): a thread sums several nodes
+  for (int n = t; n < Np; n += NT)
   {
-    const int i = t % Nq, j = (t / Nq) % Nq, k = t / (Nq * Nq);
+    const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
     const double wn = w[i] * w[j] * (DIM == 3 ? w[k] : 1.0);
-    const size_t id = (size_t)e * Np + t;
+    const size_t id = (size_t)e * Np + n;
     const double rho = 1.0 / me.irho, la = me.lam, mu = me.mu;
     double kin = 0, pot = 0;
     for (int a = 0; a < DIM; ++a)
@@ -50,7 +51,7 @@ __global__ void __launch_bounds__(Shape<DIM, N>::NT)
       pot = (aa * sxx * sxx - 2 * bb * sxx * syy + aa * syy * syy) / det +
             sxy * sxy / mu;
     }
-    val = wn * (kin + pot);
+    val += wn * (kin + pot);
   }
   for (int o = 16; o > 0; o >>= 1)
     val += __shfl_down_sync(0xffffffffu, val, o);

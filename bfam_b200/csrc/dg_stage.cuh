@@ -198,15 +198,18 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
     const int k = ds.y & 3;
     if (k == 2)
       continue;
-    const int nface = (ds.y >> 2) & 7;
-    const int src_n =
-        k == 0 ? gmask<DIM, N>(nface, face_perm<DIM, N>((ds.y >> 5) & 7, pn))
-               : gmask<DIM, N>(nface, pn);
-    const double *src = d.qin + (size_t)ds.x * Np + src_n;
-    double *dst = pt + f * NFLD * Nfp + pn;
+    if (k != 3) // a boundary face's ghost trace comes from the element itself
+    {
+      const int nface = (ds.y >> 2) & 7;
+      const int src_n =
+          k == 0 ? gmask<DIM, N>(nface, face_perm<DIM, N>((ds.y >> 5) & 7, pn))
+                 : gmask<DIM, N>(nface, pn);
+      const double *src = d.qin + (size_t)ds.x * Np + src_n;
+      double *dst = pt + f * NFLD * Nfp + pn;
 #pragma unroll
-    for (int c = 0; c < NTF; ++c)
-      cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
+      for (int c = 0; c < NTF; ++c)
+        cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
+    }
     if (pn == 0)
     {
       const double *fc =
@@ -342,9 +345,17 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int pp = k == 1 ? map_op<DIM, N>((y >> 5) & 7, pn) : pn;
         CT dq[NTF], J[6];
         const double *x = pt + f * NFLD * Nfp;
+        // boundary faces: ghost state v+ = v-, S+ = -S- (free surface) or
+        // q+ = 0 (absorbing)
+        const bool free_surface = k == 3 && ((y >> 2) & 3) == 0;
 #pragma unroll
         for (int c = 0; c < NTF; ++c)
-          dq[c] = CT(x[c * Nfp + pp] - qs[trace_field<DIM>(f >> 1, c) * Np + vm]);
+        {
+          const double qm = qs[trace_field<DIM>(f >> 1, c) * Np + vm];
+          const double qp = k != 3 ? x[c * Nfp + pp]
+                                   : (free_surface ? (c < DIM ? qm : -qm) : 0.0);
+          dq[c] = CT(qp - qm);
+        }
         const CT sg = (f & 1) ? CT(1) : CT(-1);
         flux_jumps<DIM, CT>(dq, f >> 1, sg, CT(me.Zp), CT(me.Zs),
                             fcf + 4 * f, sp.flux, J);

@@ -98,6 +98,8 @@ void bfam_b200_brick_mesh_free(bfam_b200_mesh_t *m)
   free(m->vmapP);
   free(m->EToEm);
   free(m->EToFm);
+  free(m->EToEb);
+  free(m->EToFb);
   free(m->EToHm);
   free(m->EToEp);
   free(m->EToHp);
@@ -119,8 +121,6 @@ int bfam_b200_brick_mesh_new(const bfam_b200_brick_spec_t *spec,
   {
     if (n[a] < 1 || n[a] > (1 << 20))
       return 3;
-    if (!spec->periodic[a])
-      return 4; /* boundary glue grids are not built by this mesher */
   }
   const int64_t ncell64 = (int64_t)n[0] * n[1] * n[2];
   if (ncell64 * (dim == 3 ? 8 : 4) > INT32_MAX / 2)
@@ -216,6 +216,9 @@ int bfam_b200_brick_mesh_new(const bfam_b200_brick_spec_t *spec,
   /* neighbour search; pass 0 counts glue, pass 1 fills */
   int32_t *glue_first = malloc(sizeof(int32_t) * NF * K);
   int32_t Kg = 0;
+  m->EToEb = malloc(sizeof(int32_t) * NF * (size_t)K);
+  m->EToFb = malloc(sizeof(int8_t) * NF * (size_t)K);
+  m->Kb = 0;
   for (int pass = 0; pass < 2; ++pass)
   {
     int32_t g = 0;
@@ -240,6 +243,22 @@ int bfam_b200_brick_mesh_new(const bfam_b200_brick_spec_t *spec,
         const int32_t cn = nb[0] + n[0] * (nb[1] + n[1] * nb[2]);
         if (pass == 0)
           glue_first[NF * e + f] = -1;
+        /* a face on a non-periodic side of the brick: the element's base
+         * cell touches that side and the face is not toward a sibling */
+        const int outer = echild[e] < 0 || (s ? cc[a] == 1 : cc[a] == 0);
+        if (!spec->periodic[a] && outer &&
+            (s ? bc[a] == n[a] - 1 : bc[a] == 0))
+        {
+          m->EToE[NF * e + f] = e;
+          m->EToF[NF * e + f] = (int8_t)f;
+          if (pass == 1)
+          {
+            m->EToEb[m->Kb] = e;
+            m->EToFb[m->Kb] = (int8_t)f;
+            ++m->Kb;
+          }
+          continue;
+        }
         if (echild[e] < 0)
         {
           if (!refined[cn])

@@ -78,7 +78,7 @@ typedef struct
   int N;             /* polynomial order */
   int n[3];          /* base cells per axis (n[2] ignored in 2D) */
   double L[3];       /* domain extent per axis */
-  int periodic[3];   /* must be 1 on every axis (boundary glue not built) */
+  int periodic[3];   /* 0: the two sides of the axis are domain boundaries */
   double refine_prob; /* probability that a base cell is refined */
   uint64_t seed;     /* PCG32 seed; the refinement draw uses stream 1 */
   const uint8_t *refine_flags; /* optional explicit flags per base cell in
@@ -111,6 +111,12 @@ typedef struct
   int8_t *EToHp;
   int8_t *EToOp;
   int32_t num_refined; /* refined base cells */
+  /* boundary faces of non-periodic axes (the minus side of bfam's boundary
+   * glue, src/bfam.c:7851-7899), in (element, face) order; their vmapP
+   * points to the element itself */
+  int32_t Kb;
+  int32_t *EToEb;
+  int8_t *EToFb;
 } bfam_b200_mesh_t;
 
 /* Returns 0 on success, nonzero (and *out = NULL) on bad input. */

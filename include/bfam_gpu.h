@@ -114,6 +114,26 @@ typedef struct
   int device;            /* CUDA device ordinal */
 } bfam_gpu_options_t;
 
+/* Boundary faces of a non-periodic mesh: the minus side of bfam's boundary
+ * glue subdomain (`_glue_boundary`, src/bfam.c:7851-7899; bfam builds the
+ * grid but leaves the condition to the application), one entry per face
+ * whose vmapP points to the element itself, with the condition imposed
+ * there through the upwind flux against a ghost state:
+ *   free surface (traction-free): v+ = v-, S+ n = -S- n  (T* = 0);
+ *   absorbing (characteristic):   v+ = 0, S+ = 0 with the same material. */
+enum
+{
+  BFAM_GPU_BC_FREE_SURFACE = 0,
+  BFAM_GPU_BC_ABSORBING = 1
+};
+typedef struct
+{
+  int32_t K;            /* boundary faces */
+  const int32_t *EToE;  /* element of each face */
+  const int8_t *EToF;   /* face of that element */
+  const int8_t *type;   /* BFAM_GPU_BC_* */
+} bfam_gpu_boundary_t;
+
 typedef struct bfam_gpu_domain bfam_gpu_domain_t;
 typedef struct bfam_ts_lsrk bfam_ts_lsrk_t;
 
@@ -124,6 +144,13 @@ int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
                            const bfam_gpu_glue_t *glue,
                            const bfam_gpu_options_t *opts,
                            bfam_gpu_domain_t **out);
+/* The same with the boundary faces of a non-periodic mesh (bnd may be NULL;
+ * then every face must have a neighbour or a glue element). */
+int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
+                                         const bfam_gpu_glue_t *glue,
+                                         const bfam_gpu_boundary_t *bnd,
+                                         const bfam_gpu_options_t *opts,
+                                         bfam_gpu_domain_t **out);
 int bfam_gpu_domain_free(bfam_gpu_domain_t *dom);
 
 /* Number of fields (5 in 2D: vx vy sxx syy sxy; 9 in 3D: vx vy vz sxx syy

@@ -249,6 +249,10 @@ typedef struct
   int32_t src_elem;
   double *src_W;
   double src_force[3], src_f0, src_t0;
+  /* non-periodic axes: the brick's sides carry a boundary condition,
+   * bc[side] (sides -x, +x, -y, +y, -z, +z): 0 free surface, 1 absorbing */
+  int periodic[3];
+  int bc[6];
 } oracle_t;
 
 static int32_t owner_at(const oracle_t *o, int x, int y, int z)
@@ -276,6 +280,8 @@ oracle_t *oracle_new(int dim, int N, int32_t K, const int32_t *ecoord,
   o->K = K;
   o->flux = flux;
   o->src_elem = -1;
+  for (int a = 0; a < 3; ++a)
+    o->periodic[a] = 1;
   o->ec = ecoord;
   for (int a = 0; a < 3; ++a)
   {
@@ -432,6 +438,18 @@ int oracle_sample(const oracle_t *o, const double *q, int nrecv,
   }
   free(phi);
   return 0;
+}
+
+/* Sides of the brick on axes with periodic[a] == 0 become boundaries with
+ * condition bc[2a + side]; the ghost state is v+ = v-, S+ = -S- (free
+ * surface: zero traction) or q+ = 0 (absorbing), with the element's own
+ * material. */
+void oracle_set_boundary(oracle_t *o, const int *periodic, const int *bc)
+{
+  for (int a = 0; a < 3; ++a)
+    o->periodic[a] = a < o->dim ? periodic[a] : 1;
+  for (int f = 0; f < 6; ++f)
+    o->bc[f] = bc[f];
 }
 
 /* volume node of face node q on face f */
@@ -663,6 +681,28 @@ static void element_rhs(const oracle_t *o, const double *q, int32_t e,
     /* finest cell just outside the face, at the lower tangential corner */
     int p[3] = {ce[0], ce[1], ce[2]};
     p[a] = side ? ce[a] + s : ce[a] - 1;
+    if (!o->periodic[a] && (p[a] < 0 || p[a] >= o->D[a]))
+    {
+      /* boundary face: ghost state from the element's own trace */
+      face_trace(o, q, e, f, trm);
+      const int free_surface = o->bc[f] == 0;
+      double qm[9], qp[9], dT[3], dv[3];
+      for (int pt = 0; pt < Nfp; ++pt)
+      {
+        for (int c = 0; c < NFLD; ++c)
+        {
+          qm[c] = trm[c * Nfp + pt];
+          qp[c] = free_surface ? (c < dim ? qm[c] : -qm[c]) : 0.0;
+        }
+        jumps(o, qm, qp, nrm, rho, la, mu, rho, la, mu, dT, dv);
+        for (int k = 0; k < 3; ++k)
+        {
+          Jf[k * Nfp + pt] = dT[k];
+          Jf[(3 + k) * Nfp + pt] = dv[k];
+        }
+      }
+      goto lift;
+    }
     const int32_t nb = owner_at(o, p[0], p[1], p[2]);
     const int32_t *cn = o->ec + 4 * nb;
     const int sn = cn[3];
@@ -749,6 +789,7 @@ static void element_rhs(const oracle_t *o, const double *q, int32_t e,
       }
     }
     /* lift with the lumped LGL mass: factor (2/h_normal) / w_end */
+  lift:;
     const double Lf = rx[a] / wend;
     for (int pt = 0; pt < Nfp; ++pt)
     {

@@ -38,6 +38,7 @@ def lib() -> C.CDLL:
         L.oracle_lsrk_from.argtypes = [C.c_void_p, dp, C.c_double, C.c_double, C.c_int,
                                        C.c_int, C.c_int]
         L.oracle_set_source.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_double]
+        L.oracle_set_boundary.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.oracle_sample.argtypes = [C.c_void_p, dp, C.c_int, dp, dp]
         L.oracle_energy.restype = C.c_double
         L.oracle_energy.argtypes = [C.c_void_p, dp]
@@ -91,8 +92,22 @@ class Oracle:
         self._h = h
 
     @classmethod
-    def from_mesh(cls, mesh, rho, lam, mu, flux=0):
-        return cls(mesh.dim, mesh.N, mesh.ecoord, mesh.nbase, mesh.L, rho, lam, mu, flux)
+    def from_mesh(cls, mesh, rho, lam, mu, flux=0, bc=0):
+        """bc: condition on the sides of a mesh's non-periodic axes, one value
+        for all or one per side (-x, +x, -y, +y[, -z, +z]); 0 free surface,
+        1 absorbing"""
+        o = cls(mesh.dim, mesh.N, mesh.ecoord, mesh.nbase, mesh.L, rho, lam, mu, flux)
+        periodic = getattr(mesh, "periodic", (True, True, True))
+        if not all(periodic):
+            o.set_boundary(periodic, bc)
+        return o
+
+    def set_boundary(self, periodic, bc) -> None:
+        sides = np.broadcast_to(np.asarray(bc, dtype=np.int64), (2 * self.dim,))
+        pv = (C.c_int * 3)(*[int(bool(periodic[a])) if a < self.dim else 1
+                             for a in range(3)])
+        bv = (C.c_int * 6)(*([int(x) for x in sides] + [0] * (6 - len(sides))))
+        lib().oracle_set_boundary(self._h, pv, bv)
 
     def __del__(self):
         if getattr(self, "_h", None):

@@ -117,6 +117,19 @@ def test_energy_parity_and_decay():
     assert np.all(np.diff(E) < 0)
 
 
+@pytest.mark.parametrize("dim,N", [(2, 1), (2, 7), (3, 1), (3, 3), (3, 5), (3, 6), (3, 7)])
+def test_energy_parity_every_order(dim, N):
+    """every node counts, also where a CTA has fewer threads than nodes"""
+    m = bf.Mesh(dim, N, (2,) * dim, refine_prob=0.5, seed=N)
+    rho, lam, mu = bf.material_random(m.K, N)
+    q = np.random.default_rng(N).standard_normal((m.nfields, m.K * m.Np))
+    dom = bf.GpuDomain(m, rho, lam, mu)
+    dom.set_fields(q)
+    ref = orc.Oracle.from_mesh(m, rho, lam, mu).energy(q)
+    assert abs(dom.energy() - ref) < 1e-12 * ref
+    assert abs(dom.energy_noalloc() - ref) < 1e-12 * ref
+
+
 def test_plane_wave_converges_on_gpu():
     """Analytic P wave through nested meshes with mortars: order ~N+1."""
     N, k, T = 3, (2 * math.pi, 0.0, 0.0), 0.05
