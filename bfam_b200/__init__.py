@@ -21,6 +21,7 @@ FIELDS_3D = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
 
 FLUX_UPWIND, FLUX_CENTRAL = 0, 1
 BC_FREE_SURFACE, BC_ABSORBING = 0, 1
+NQUAD = 5  # tree, level, x, y, z per element (BFAM_GPU_NQUAD)
 # status codes of the C-ABI
 (BFAM_GPU_EINVAL, BFAM_GPU_ENOMEM, BFAM_GPU_ECUDA, BFAM_GPU_ETIMEOUT,
  BFAM_GPU_EUNSUPPORTED) = (-1, -2, -3, -4, -5)
@@ -89,6 +90,11 @@ class BoundaryDesc(C.Structure):
     _fields_ = [("K", C.c_int32), ("EToE", i32p), ("EToF", i8p), ("type", i8p)]
 
 
+class QuadrantsDesc(C.Structure):
+    _fields_ = [("num_trees", C.c_int32), ("tree_x0", dp), ("tree_h", dp),
+                ("quads", i32p), ("root_len", C.c_int32)]
+
+
 class SourceDesc(C.Structure):
     _fields_ = [("x", C.c_double * 3), ("force", C.c_double * 3),
                 ("f0", C.c_double), ("t0", C.c_double)]
@@ -122,6 +128,10 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_domain_create_with_boundary": (C.c_int, [P(VolumeDesc), P(GlueDesc),
                                                            P(BoundaryDesc), P(Options),
                                                            P(vp)]),
+        "bfam_gpu_domain_create_from_quadrants": (C.c_int, [P(VolumeDesc), P(GlueDesc),
+                                                            P(BoundaryDesc), P(QuadrantsDesc),
+                                                            P(Options), P(vp)]),
+        "bfam_gpu_domain_get_geometry": (C.c_int, [vp, dp, dp]),
         "bfam_gpu_domain_free": (C.c_int, [vp]),
         "bfam_gpu_domain_num_fields": (C.c_int, [vp]),
         "bfam_gpu_domain_field_length": (C.c_size_t, [vp]),
@@ -315,6 +325,30 @@ class Mesh:
     def empty_fields(self) -> np.ndarray:
         return np.zeros((self.nfields, self.K * self.Np))
 
+    def quadrants(self, root_len: int | None = None):
+        """p4est's view of the mesh: one tree per base cell (numbered x
+        fastest), tree boxes [T][3] (lower corner, edge lengths), and per
+        element (tree, level, x, y, z) in integer coordinates of [0,
+        root_len) (P4EST_ROOT_LEN: 2^30 in 2D, 2^19 in 3D)."""
+        root = root_len or (1 << (19 if self.dim == 3 else 30))
+        n = np.array(self.nbase[:3])
+        unit = np.array(self.L[:3]) / n
+        T = int(np.prod(n))
+        t = np.arange(T)
+        b = np.stack([t % n[0], (t // n[0]) % n[1], t // (n[0] * n[1])], axis=1)
+        tree_x0 = np.ascontiguousarray(b * unit, dtype=np.float64)
+        tree_h = np.ascontiguousarray(np.broadcast_to(unit, (T, 3)), dtype=np.float64)
+        ec = self.ecoord.astype(np.int64)
+        base = ec[:, :3] // 2
+        tree = base[:, 0] + n[0] * (base[:, 1] + n[1] * base[:, 2])
+        level = np.where(ec[:, 3] == 2, 0, 1)
+        xyz = (ec[:, :3] - 2 * base) * (root // 2)
+        if self.dim == 2:
+            xyz[:, 2] = 0
+        quads = np.ascontiguousarray(
+            np.column_stack([tree, level, xyz]).astype(np.int32))
+        return tree_x0, tree_h, quads, root
+
     def plane_wave(self, r, k, amplitude, rho, lam, mu, time=0.0) -> np.ndarray:
         q = self.empty_fields()
         kv = np.zeros(3)
@@ -348,9 +382,11 @@ class GpuDomain:
 
     def __init__(self, mesh: Mesh, rho, lam, mu, flux: int = FLUX_UPWIND,
                  precision: int = PRECISION_FP64, mem_budget_bytes: int = 0,
-                 device: int = 0, bc=BC_FREE_SURFACE):
+                 device: int = 0, bc=BC_FREE_SURFACE, geometry: str = "host"):
         """bc: the condition on the boundary faces of a non-periodic mesh,
-        one value for every side or one per side (-x, +x, -y, +y, -z, +z)"""
+        one value for every side or one per side (-x, +x, -y, +y, -z, +z);
+        geometry "host": element boxes uploaded (x0, h); "device": computed
+        on the GPU from the mesh's quadrant data"""
         L = lib()
         self.mesh = mesh
         N = mesh.N
@@ -388,6 +424,8 @@ class GpuDomain:
         opt.flux, opt.precision = flux, precision
         opt.mem_budget_bytes, opt.device = mem_budget_bytes, device
         h = C.c_void_p()
+        self.bc = None
+        bnd = None
         if getattr(mesh, "Kb", 0):
             sides = np.broadcast_to(np.asarray(bc, dtype=np.int8), (2 * mesh.dim,))
             btype = np.ascontiguousarray(sides[mesh.EToFb], dtype=np.int8)
@@ -398,10 +436,23 @@ class GpuDomain:
             bnd.EToF = mesh.EToFb.ctypes.data_as(i8p)
             bnd.type = btype.ctypes.data_as(i8p)
             self.bc = tuple(int(x) for x in sides)
+        if geometry == "device":
+            tx0, th, quads, root = mesh.quadrants()
+            self._keep += [tx0, th, quads]
+            qd = QuadrantsDesc()
+            qd.num_trees, qd.root_len = len(tx0), root
+            qd.tree_x0, qd.tree_h = _dp(tx0), _dp(th)
+            qd.quads = quads.ctypes.data_as(i32p)
+            vol.x0, vol.h = dp(), dp()
+            _check(L.bfam_gpu_domain_create_from_quadrants(
+                C.byref(vol), C.byref(glue), C.byref(bnd) if bnd else None, C.byref(qd),
+                C.byref(opt), C.byref(h)))
+        elif geometry != "host":
+            raise ValueError(f"geometry must be 'host' or 'device' (got {geometry!r})")
+        elif bnd is not None:
             _check(L.bfam_gpu_domain_create_with_boundary(
                 C.byref(vol), C.byref(glue), C.byref(bnd), C.byref(opt), C.byref(h)))
         else:
-            self.bc = None
             _check(L.bfam_gpu_domain_create(C.byref(vol), C.byref(glue), C.byref(opt),
                                             C.byref(h)))
         self._h = h
@@ -411,6 +462,13 @@ class GpuDomain:
     @property
     def handle(self):
         return self._h
+
+    def geometry(self):
+        """element boxes the domain computes with: x0, h, [K][3] each"""
+        K = self.mesh.K
+        x0, h = np.zeros((K, 3)), np.zeros((K, 3))
+        _check(lib().bfam_gpu_domain_get_geometry(self._h, _dp(x0), _dp(h)))
+        return x0, h
 
     def free(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -458,6 +458,8 @@ int bfam_gpu_domain_set_source(bfam_gpu_domain_t *d,
     ++d->extras_gen;
     return 0;
   }
+  if (int rc = host_geometry(d))
+    return rc;
   double xi[3];
   const int e = locate(d, src->x, xi);
   if (e < 0)
@@ -501,6 +503,8 @@ int bfam_gpu_domain_set_receivers(bfam_gpu_domain_t *d, int nrecv,
     return fail(BFAM_GPU_EINVAL, "bad receiver arguments");
   CUDA_TRY(cudaSetDevice(d->device));
   CUDA_TRY(cudaStreamSynchronize(d->stream));
+  if (int rc = host_geometry(d))
+    return rc;
   std::vector<int> elem(nrecv);
   std::vector<double> w((size_t)nrecv * d->Np);
   for (int r = 0; r < nrecv; ++r)

@@ -6,6 +6,7 @@
 // stage kernel once per LSRK stage (optionally replayed from a CUDA graph).
 #include "bfam_gpu.h"
 #include "dg_energy.cuh"
+#include "dg_geometry.cuh"
 #include "dg_stage.cuh"
 #include "gpu_internal.h"
 
@@ -222,6 +223,22 @@ void dev_free(bfam_gpu_domain_t *d, void *p)
     }
 }
 
+int host_geometry(bfam_gpu_domain_t *d)
+{
+  if (!d->hx0.empty() || !d->gx0)
+    return 0;
+  std::vector<double> x0(3 * (size_t)d->K), h(3 * (size_t)d->K);
+  CUDA_TRY(cudaSetDevice(d->device));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  CUDA_TRY(cudaMemcpy(x0.data(), d->gx0, sizeof(double) * x0.size(),
+                      cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(h.data(), d->gh, sizeof(double) * h.size(),
+                      cudaMemcpyDeviceToHost));
+  d->hx0.swap(x0);
+  d->hh.swap(h);
+  return 0;
+}
+
 void release(bfam_gpu_domain_t *d)
 {
   if (!d)
@@ -310,6 +327,13 @@ int bfam_gpu_last_error(char *buf, size_t len)
 
 uint64_t bfam_gpu_launch_count(void) { return g_launches.load(); }
 
+static int create_domain(const bfam_gpu_volume_t *vol,
+                         const bfam_gpu_glue_t *glue,
+                         const bfam_gpu_boundary_t *bnd,
+                         const bfam_gpu_quadrants_t *quads,
+                         const bfam_gpu_options_t *opts,
+                         bfam_gpu_domain_t **out);
+
 int bfam_gpu_domain_create(const bfam_gpu_volume_t *vol,
                            const bfam_gpu_glue_t *glue,
                            const bfam_gpu_options_t *opts,
@@ -323,6 +347,78 @@ int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
                                          const bfam_gpu_boundary_t *bnd,
                                          const bfam_gpu_options_t *opts,
                                          bfam_gpu_domain_t **out)
+{
+  return create_domain(vol, glue, bnd, nullptr, opts, out);
+}
+
+int bfam_gpu_domain_create_from_quadrants(const bfam_gpu_volume_t *vol,
+                                          const bfam_gpu_glue_t *glue,
+                                          const bfam_gpu_boundary_t *bnd,
+                                          const bfam_gpu_quadrants_t *quads,
+                                          const bfam_gpu_options_t *opts,
+                                          bfam_gpu_domain_t **out)
+{
+  if (out)
+    *out = nullptr;
+  if (!quads)
+    return fail(BFAM_GPU_EINVAL, "quads is NULL");
+  return create_domain(vol, glue, bnd, quads, opts, out);
+}
+
+namespace
+{
+
+// quadrant data: trees are boxes, every element a quadrant of its tree
+int check_quadrants(const bfam_gpu_quadrants_t *qd, int dim, int32_t K)
+{
+  if (!qd->tree_x0 || !qd->tree_h || !qd->quads)
+    return fail(BFAM_GPU_EINVAL, "a required quadrant array is NULL");
+  const int32_t root = qd->root_len;
+  if (root < 1 || root > (1 << 30) || (root & (root - 1)))
+    return fail(BFAM_GPU_EINVAL, "root_len %d is not a power of two <= 2^30",
+                root);
+  if (qd->num_trees < 1)
+    return fail(BFAM_GPU_EINVAL, "num_trees must be positive (got %d)",
+                qd->num_trees);
+  for (int32_t t = 0; t < qd->num_trees; ++t)
+    for (int a = 0; a < dim; ++a)
+    {
+      const double x = qd->tree_x0[3 * (size_t)t + a],
+                   h = qd->tree_h[3 * (size_t)t + a];
+      if (!std::isfinite(x) || !std::isfinite(h) || !(h > 0))
+        return fail(BFAM_GPU_EINVAL, "tree %d: bad box on axis %d", t, a);
+    }
+  int maxlevel = 0;
+  while ((1 << maxlevel) < root)
+    ++maxlevel;
+  for (int32_t e = 0; e < K; ++e)
+  {
+    const int32_t *q = qd->quads + BFAM_GPU_NQUAD * (size_t)e;
+    if (q[0] < 0 || q[0] >= qd->num_trees)
+      return fail(BFAM_GPU_EINVAL, "element %d: tree %d out of range", e,
+                  q[0]);
+    if (q[1] < 0 || q[1] > maxlevel)
+      return fail(BFAM_GPU_EINVAL, "element %d: level %d out of [0, %d]", e,
+                  q[1], maxlevel);
+    const int32_t len = root >> q[1];
+    for (int a = 0; a < dim; ++a)
+      if (q[2 + a] < 0 || q[2 + a] >= root || q[2 + a] % len)
+        return fail(BFAM_GPU_EINVAL,
+                    "element %d: coordinate %d on axis %d is not a level-%d "
+                    "quadrant corner in [0, %d)",
+                    e, q[2 + a], a, q[1], root);
+  }
+  return 0;
+}
+
+} // namespace
+
+static int create_domain(const bfam_gpu_volume_t *vol,
+                         const bfam_gpu_glue_t *glue,
+                         const bfam_gpu_boundary_t *bnd,
+                         const bfam_gpu_quadrants_t *quads,
+                         const bfam_gpu_options_t *opts,
+                         bfam_gpu_domain_t **out)
 {
   if (!out)
     return fail(BFAM_GPU_EINVAL, "out is NULL");
@@ -342,8 +438,11 @@ int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
     return fail(BFAM_GPU_EUNSUPPORTED, "order N=%d in %dD is not compiled in",
                 N, dim);
   if (!vol->r || !vol->w || !vol->Dr || !vol->vmapM || !vol->vmapP ||
-      !vol->x0 || !vol->h || !vol->rho || !vol->lambda || !vol->mu)
+      (!quads && (!vol->x0 || !vol->h)) || !vol->rho || !vol->lambda ||
+      !vol->mu)
     return fail(BFAM_GPU_EINVAL, "a required volume array is NULL");
+  if (quads && check_quadrants(quads, dim, vol->K))
+    return BFAM_GPU_EINVAL;
   if (opts->flux != BFAM_GPU_FLUX_UPWIND && opts->flux != BFAM_GPU_FLUX_CENTRAL)
     return fail(BFAM_GPU_EINVAL, "unknown flux %d", opts->flux);
 
@@ -654,6 +753,8 @@ int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
     x.mu = mu;
     x.Zp = std::sqrt(rho * (la + 2 * mu));
     x.Zs = std::sqrt(rho * mu);
+    if (quads)
+      continue; // the metric comes from the device geometry kernel
     for (int a = 0; a < 3; ++a)
     {
       const double h = a < dim ? vol->h[3 * e + a] : 1.0;
@@ -754,10 +855,41 @@ int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
   TRY(upload(d, &d->ops, ops.data(), ops.size()));
   TRY(dev_alloc(d, (void **)&d->err, sizeof(int)));
   TRY(dev_alloc(d, (void **)&d->clock, sizeof(DomainClock)));
+  if (quads)
+  {
+    // element boxes and metric on the device; the quadrant and tree tables
+    // are needed only here
+    int32_t *dq = nullptr;
+    double *tx0 = nullptr, *th = nullptr;
+    TRY(upload(d, &dq, quads->quads, (size_t)BFAM_GPU_NQUAD * K));
+    TRY(upload(d, &tx0, quads->tree_x0, 3 * (size_t)quads->num_trees));
+    TRY(upload(d, &th, quads->tree_h, 3 * (size_t)quads->num_trees));
+    TRY(dev_alloc(d, (void **)&d->gx0, 3 * sizeof(double) * (size_t)K));
+    TRY(dev_alloc(d, (void **)&d->gh, 3 * sizeof(double) * (size_t)K));
+    dg_geometry_kernel<<<(K + 255) / 256, 256, 0, d->stream>>>(
+        K, dim, dq, tx0, th, 1.0 / quads->root_len, d->ed, d->gx0, d->gh);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess)
+      ce = cudaStreamSynchronize(d->stream);
+    dev_free(d, dq);
+    dev_free(d, tx0);
+    dev_free(d, th);
+    if (ce != cudaSuccess)
+    {
+      release(d);
+      return fail(BFAM_GPU_ECUDA, "geometry kernel: %s",
+                  cudaGetErrorString(ce));
+    }
+  }
 #undef TRY
-  // host copies for locating sources and receivers
-  d->hx0.assign(vol->x0, vol->x0 + 3 * (size_t)vol->K);
-  d->hh.assign(vol->h, vol->h + 3 * (size_t)vol->K);
+  // host copies for locating sources and receivers (device geometry: read
+  // back when first needed)
+  if (!quads)
+  {
+    d->hx0.assign(vol->x0, vol->x0 + 3 * (size_t)vol->K);
+    d->hh.assign(vol->h, vol->h + 3 * (size_t)vol->K);
+  }
   d->hr.assign(vol->r, vol->r + d->Nq);
   d->hw.assign(vol->w, vol->w + d->Nq);
   if (cudaMemset(d->q[0], 0, state) != cudaSuccess ||
@@ -771,6 +903,20 @@ int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
   }
   (void)nmap;
   *out = d;
+  return 0;
+}
+
+int bfam_gpu_domain_get_geometry(bfam_gpu_domain_t *d, double *x0, double *h)
+{
+  if (!d)
+    return fail(BFAM_GPU_EINVAL, "NULL domain");
+  const int rc = host_geometry(d);
+  if (rc)
+    return rc;
+  if (x0)
+    std::memcpy(x0, d->hx0.data(), sizeof(double) * d->hx0.size());
+  if (h)
+    std::memcpy(h, d->hh.data(), sizeof(double) * d->hh.size());
   return 0;
 }
 

@@ -106,6 +106,9 @@ struct bfam_gpu_domain
   // host copies for locating sources and receivers: element lower corners
   // and edge lengths [K][3], LGL nodes and weights [Nq]
   std::vector<double> hx0, hh, hr, hw;
+  // element boxes computed on the device from quadrant data ([K][3] each;
+  // null when the boxes came from the host)
+  double *gx0 = nullptr, *gh = nullptr;
   // time-dependent extras: device clock, Ricker point source, receivers
   bfam_b200::DomainClock *clock = nullptr;
   bool clock_valid = false; // device clock holds the stepper's time
@@ -137,6 +140,9 @@ namespace host
 
 // device allocation counted against the domain's budget, freed with it
 int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes);
+// fills the host copies of the element boxes (read back from the device
+// when the domain computed them from quadrant data)
+int host_geometry(bfam_gpu_domain_t *d);
 // frees one allocation made by dev_alloc before the domain is freed
 void dev_free(bfam_gpu_domain_t *d, void *p);
 

@@ -151,6 +151,45 @@ int bfam_gpu_domain_create_with_boundary(const bfam_gpu_volume_t *vol,
                                          const bfam_gpu_boundary_t *bnd,
                                          const bfam_gpu_options_t *opts,
                                          bfam_gpu_domain_t **out);
+
+/* Element geometry from p4est quadrant data, computed on the device: the
+ * per-element layout bfam's device kernels were given for this purpose
+ * (ID_QUAD_TID, ID_QUAD_LVL, ID_QUAD_X/Y/Z, NQUAD and QUAD_ROOT_LEN,
+ * src/bfam.h:1600-1606, src/bfam.c:8697-8705).  Element e lies in tree
+ * t = quads[NQUAD e + 0] at level l = quads[NQUAD e + 1] with integer lower
+ * corner (x, y, z) = quads[NQUAD e + 2 .. 4] in [0, root_len); its box is
+ *   x0_a = tree_x0[3 t + a] + tree_h[3 t + a] * (x_a / root_len),
+ *   h_a  = tree_h[3 t + a] * 2^-l.
+ * Trees are affine boxes (a brick connectivity's trees after the
+ * application's coordinate map): tree_x0/tree_h are their lower corners and
+ * edge lengths, one row per tree. */
+enum
+{
+  BFAM_GPU_NQUAD = 5
+};
+typedef struct
+{
+  int32_t num_trees;
+  const double *tree_x0;  /* [num_trees][3] */
+  const double *tree_h;   /* [num_trees][3], > 0 on the mesh's axes */
+  const int32_t *quads;   /* [K][BFAM_GPU_NQUAD]: tree, level, x, y, z */
+  int32_t root_len;       /* P4EST_ROOT_LEN: a power of two, <= 2^30 */
+} bfam_gpu_quadrants_t;
+
+/* bfam_gpu_domain_create_with_boundary with the element boxes computed on
+ * the device from quads (vol->x0 and vol->h are not read and may be NULL):
+ * the host uploads 20 bytes per element instead of 48 and computes no
+ * per-element geometry. */
+int bfam_gpu_domain_create_from_quadrants(const bfam_gpu_volume_t *vol,
+                                          const bfam_gpu_glue_t *glue,
+                                          const bfam_gpu_boundary_t *bnd,
+                                          const bfam_gpu_quadrants_t *quads,
+                                          const bfam_gpu_options_t *opts,
+                                          bfam_gpu_domain_t **out);
+/* The element boxes the domain computes with: lower corners and edge
+ * lengths, [K][3] each (either may be NULL). */
+int bfam_gpu_domain_get_geometry(bfam_gpu_domain_t *dom, double *x0,
+                                 double *h);
 int bfam_gpu_domain_free(bfam_gpu_domain_t *dom);
 
 /* Number of fields (5 in 2D: vx vy sxx syy sxy; 9 in 3D: vx vy vz sxx syy
