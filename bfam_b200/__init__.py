@@ -20,7 +20,7 @@ FIELDS_2D = ("vx", "vy", "sxx", "syy", "sxy")
 FIELDS_3D = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "sxz", "syz")
 
 FLUX_UPWIND, FLUX_CENTRAL = 0, 1
-BC_FREE_SURFACE, BC_ABSORBING = 0, 1
+BC_FREE_SURFACE, BC_ABSORBING, BC_GLUED = 0, 1, 2
 NQUAD = 5  # tree, level, x, y, z per element (BFAM_GPU_NQUAD)
 # status codes of the C-ABI
 (BFAM_GPU_EINVAL, BFAM_GPU_ENOMEM, BFAM_GPU_ECUDA, BFAM_GPU_ETIMEOUT,
@@ -95,6 +95,11 @@ class QuadrantsDesc(C.Structure):
                 ("quads", i32p), ("root_len", C.c_int32)]
 
 
+class PGlueDesc(C.Structure):
+    _fields_ = [("K", C.c_int32), ("bm", i32p), ("bp", i32p), ("N_g", C.c_int),
+                ("I_m2g", dp), ("P_g2m", dp), ("I_p2g", dp), ("P_g2p", dp)]
+
+
 class SourceDesc(C.Structure):
     _fields_ = [("x", C.c_double * 3), ("force", C.c_double * 3),
                 ("f0", C.c_double), ("t0", C.c_double)]
@@ -157,6 +162,9 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_batch_time": (C.c_int, [vp, C.c_int, dp]),
         "bfam_gpu_batch_sync": (C.c_int, [vp]),
         "bfam_gpu_batch_free": (C.c_int, [vp]),
+        "bfam_gpu_pglue_create": (C.c_int, [vp, vp, P(PGlueDesc), P(vp)]),
+        "bfam_gpu_pglue_free": (C.c_int, [vp]),
+        "bfam_gpu_batch_add_pglue": (C.c_int, [vp, vp]),
         "bfam_gpu_batch_launches_per_step": (C.c_int, [vp]),
         "bfam_gpu_domain_launch_levels": (C.c_int, [vp]),
         "bfam_gpu_batch_num_groups": (C.c_int, [vp]),
@@ -593,6 +601,11 @@ class Batch:
                                    dtype=np.float64)
         _check(lib().bfam_gpu_batch_step(self._h, _dp(dts), nsteps, 1 if use_graph else 0))
 
+    def add_pglue(self, g: "PGlue") -> None:
+        """step the glue with the batch (bfam_gpu_batch_add_pglue)"""
+        _check(lib().bfam_gpu_batch_add_pglue(self._h, g.handle))
+        self._glues = getattr(self, "_glues", []) + [g]
+
     def time(self, i: int) -> float:
         t = C.c_double()
         _check(lib().bfam_gpu_batch_time(self._h, i, C.byref(t)))
@@ -654,6 +667,82 @@ class LSRK:
     def free(self):
         if getattr(self, "_h", None) and self._h.value:
             lib().bfam_ts_lsrk_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------ glue between two domains
+
+def glued_x_pairs(ma: Mesh, mb: Mesh):
+    """Boundary-list entries pairing two bricks that share their y/z extent
+    and are glued along x into one periodic domain: a's +x side to b's -x
+    side and b's +x side to a's -x side (elements meeting with the same
+    box on the face).  Returns (entries of a, entries of b)."""
+    def side(m, f):
+        out = {}
+        for k in np.flatnonzero(m.EToFb == f):
+            e = int(m.EToEb[k])
+            key = tuple(np.round(np.r_[m.x0[e, 1:m.dim], m.h[e, 1:m.dim]], 12))
+            out[key] = int(k)
+        return out
+
+    am, ap, bm, bp = side(ma, 0), side(ma, 1), side(mb, 0), side(mb, 1)
+    ea, eb = [], []
+    for s, t in ((ap, bm), (am, bp)):
+        if set(s) != set(t):
+            raise ValueError("the glued sides do not match face by face")
+        for key in sorted(s):
+            ea.append(s[key])
+            eb.append(t[key])
+    return np.array(ea, dtype=np.int32), np.array(eb, dtype=np.int32)
+
+
+class PGlue:
+    """bfam_gpu_pglue_t: glue between domain dom_m (entries bm of its
+    boundary list) and domain dom_p (entries bp), glue order Ng (default max of the two
+    orders), with bfam's operators interpolation[0] / projection[0] of each
+    side (mortar_operators(N, Ng)[0], mortar_operators(Ng, N)[0])."""
+
+    def __init__(self, dom_m: GpuDomain, dom_p: GpuDomain, bm, bp, Ng: int | None = None):
+        Nm, Np_ = dom_m.mesh.N, dom_p.mesh.N
+        Ng = Ng or max(Nm, Np_)
+        self._bm = np.ascontiguousarray(bm, dtype=np.int32)
+        self._bp = np.ascontiguousarray(bp, dtype=np.int32)
+        desc = PGlueDesc()
+        desc.K = len(self._bm)
+        desc.bm = self._bm.ctypes.data_as(i32p)
+        desc.bp = self._bp.ctypes.data_as(i32p)
+        desc.N_g = Ng
+        self._ops = []
+        for name_i, name_p, N in (("I_m2g", "P_g2m", Nm), ("I_p2g", "P_g2p", Np_)):
+            if N == Ng:
+                setattr(desc, name_i, dp())
+                setattr(desc, name_p, dp())
+                continue
+            I = np.ascontiguousarray(mortar_operators(N, Ng)[0])
+            P = np.ascontiguousarray(mortar_operators(Ng, N)[0])
+            self._ops += [I, P]
+            setattr(desc, name_i, _dp(I))
+            setattr(desc, name_p, _dp(P))
+        h = C.c_void_p()
+        _check(lib().bfam_gpu_pglue_create(dom_m.handle, dom_p.handle, C.byref(desc),
+                                           C.byref(h)))
+        self._h = h
+        self.Ng = Ng
+        self.domains = (dom_m, dom_p)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().bfam_gpu_pglue_free(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -11,6 +11,7 @@
 // CUDA graph and replayed.
 #include "bfam_gpu.h"
 #include "dg_extras.cuh"
+#include "dg_pglue.cuh"
 #include "dg_stage.cuh"
 #include "gpu_internal.h"
 
@@ -274,6 +275,23 @@ struct bfam_gpu_batch
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool views_ok = false;
   std::vector<void *> allocs;
+  // glue between domains: its two domains' indices in the batch
+  std::vector<bfam_gpu_pglue_t *> pglues;
+  std::vector<int> pglue_dom[2];
+};
+
+// Glue between two domains: per pair the glued face, its mortar slot and the
+// side's operators, on the device.
+struct bfam_gpu_pglue
+{
+  bfam_gpu_domain_t *d[2] = {nullptr, nullptr};
+  int32_t K = 0;
+  int Ng = 0, flux = 0, device = 0;
+  std::vector<int32_t> entries[2]; // boundary-list entries (host)
+  int32_t *elem[2] = {nullptr, nullptr}, *slot[2] = {nullptr, nullptr};
+  int8_t *face[2] = {nullptr, nullptr};
+  double *I[2] = {nullptr, nullptr}, *P[2] = {nullptr, nullptr};
+  std::vector<void *> allocs;
 };
 
 namespace
@@ -391,8 +409,11 @@ int upload_views(bfam_gpu_batch_t *b)
 
 // one step from batch parity p: every stage of every group, then the
 // post-step kernel over all domains
+int issue_step_glued(bfam_gpu_batch_t *b, int p);
 int issue_step(bfam_gpu_batch_t *b, int p)
 {
+  if (!b->pglues.empty())
+    return issue_step_glued(b, p);
   CUDA_TRY(cudaEventRecord(b->fork, b->stream));
   int launches = 0;
   for (auto &g : b->groups)
@@ -431,10 +452,117 @@ int issue_step(bfam_gpu_batch_t *b, int p)
 
 int launches_per_step(const bfam_gpu_batch_t *b)
 {
-  int n = 1;
+  int n = 1 + b->ns * (int)b->pglues.size();
   for (const auto &g : b->groups)
     n += b->ns * (int)g.work.size();
   return n;
+}
+
+// the coupling kernel's view of glue k at state parity par
+PGlueView pglue_view(const bfam_gpu_batch_t *b, size_t k, int par)
+{
+  const bfam_gpu_pglue_t *g = b->pglues[k];
+  PGlueView v;
+  for (int sd = 0; sd < 2; ++sd)
+  {
+    const int i = b->pglue_dom[sd][k];
+    const bfam_gpu_domain_t *d = b->doms[i];
+    PGlueSide &S = v.s[sd];
+    S.q = d->q[(b->cur0[i] + par) & 1];
+    S.fs = d->fs;
+    S.N = d->N;
+    S.ed = d->ed;
+    S.mbuf = d->mbuf;
+    S.elem = g->elem[sd];
+    S.face = g->face[sd];
+    S.slot = g->slot[sd];
+    S.I = g->I[sd];
+    S.P = g->P[sd];
+  }
+  v.K = g->K;
+  v.Ng = g->Ng;
+  v.flux = g->flux;
+  return v;
+}
+
+// With glue between domains the groups meet at every stage: the coupling
+// launches read every glued domain's stage input and fill the glued faces'
+// slots before any element launch of the stage.
+int issue_step_glued(bfam_gpu_batch_t *b, int p)
+{
+  int launches = 0;
+  for (int s = 0; s < b->ns; ++s)
+  {
+    const int par = (p + s) & 1;
+    for (size_t k = 0; k < b->pglues.size(); ++k)
+    {
+      const PGlueView v = pglue_view(b, k, par);
+      if (b->doms[0]->dim == 3)
+        dg_pglue_kernel<3><<<v.K, PGLUE_THREADS, 0, b->stream>>>(v);
+      else
+        dg_pglue_kernel<2><<<v.K, PGLUE_THREADS, 0, b->stream>>>(v);
+      CUDA_TRY(cudaGetLastError());
+      ++launches;
+    }
+    CUDA_TRY(cudaEventRecord(b->fork, b->stream));
+    for (auto &g : b->groups)
+    {
+      CUDA_TRY(cudaStreamWaitEvent(g.stream, b->fork, 0));
+      const BatchTile &t = g.tiles[g.tile];
+      StageParams sp;
+      sp.A = b->A[s];
+      sp.B = b->B[s];
+      sp.dt = 0;
+      sp.C = b->C[s];
+      sp.first_stage = s == 0;
+      sp.flux = g.flux;
+      for (size_t l = 0; l < g.work.size(); ++l)
+      {
+        t.launch(g.views[par], g.work[l], (int)g.nwork_l[l], sp,
+                 g.hops.data(), g.grid[l], g.stream);
+        CUDA_TRY(cudaGetLastError());
+        ++launches;
+      }
+      CUDA_TRY(cudaEventRecord(g.done, g.stream));
+      CUDA_TRY(cudaStreamWaitEvent(b->stream, g.done, 0));
+    }
+  }
+  dg_post_step_kernel<<<(int)b->doms.size(), POST_THREADS, 0, b->stream>>>(
+      b->post[p]);
+  CUDA_TRY(cudaGetLastError());
+  ++launches;
+  g_launches.fetch_add(launches, std::memory_order_relaxed);
+  return 0;
+}
+
+// every glued face of the batch's domains joined by exactly one of its glues,
+// and glued domains stepping with one time step
+int check_glue(const bfam_gpu_batch_t *b, const double *dt)
+{
+  const int nd = (int)b->doms.size();
+  std::vector<std::vector<int>> used(nd);
+  for (int i = 0; i < nd; ++i)
+    used[i].assign(b->doms[i]->bslot.size(), 0);
+  for (size_t k = 0; k < b->pglues.size(); ++k)
+  {
+    const int i0 = b->pglue_dom[0][k], i1 = b->pglue_dom[1][k];
+    if (dt[i0] != dt[i1] || b->t[i0] != b->t[i1])
+      return fail(BFAM_GPU_EINVAL,
+                  "glued domains %d and %d step with different times or time "
+                  "steps",
+                  i0, i1);
+    for (int sd = 0; sd < 2; ++sd)
+      for (int32_t e : b->pglues[k]->entries[sd])
+        ++used[b->pglue_dom[sd][k]][e];
+  }
+  for (int i = 0; i < nd; ++i)
+    for (size_t e = 0; e < used[i].size(); ++e)
+      if ((b->doms[i]->bslot[e] >= 0) != (used[i][e] == 1))
+        return fail(BFAM_GPU_EINVAL,
+                    "domain %d: glued face (boundary entry %zu) is joined by "
+                    "%d glues of the batch",
+                    i, e, used[i][e]);
+  return 0;
 }
 
 } // namespace
@@ -783,6 +911,8 @@ int bfam_gpu_batch_step(bfam_gpu_batch_t *b, const double *dt, int nsteps,
     return fail(BFAM_GPU_EINVAL, "bad arguments");
   CUDA_TRY(cudaSetDevice(b->device));
   const int nd = (int)b->doms.size();
+  if (int rc = check_glue(b, dt))
+    return rc;
   // the domains' buffers at the current parity, and the time steps, must be
   // those the views were built with
   bool stale = !b->views_ok;
@@ -928,6 +1058,225 @@ int bfam_gpu_batch_set_tile(bfam_gpu_batch_t *b, int g, int tile,
     choose_grid(b, G);
     return rc;
   }
+  drop_graphs(b);
+  return 0;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------- glue between domains
+
+namespace
+{
+
+void pglue_release(bfam_gpu_pglue_t *g)
+{
+  if (!g)
+    return;
+  cudaSetDevice(g->device);
+  for (void *p : g->allocs)
+    cudaFree(p);
+  delete g;
+}
+
+template <typename T>
+int pglue_upload(bfam_gpu_pglue_t *g, T **dst, const T *src, size_t n)
+{
+  cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+  if (e != cudaSuccess)
+  {
+    cudaGetLastError();
+    return fail(BFAM_GPU_ENOMEM, "glue cudaMalloc: %s", cudaGetErrorString(e));
+  }
+  g->allocs.push_back(*dst);
+  CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// a side's operators: identity (NULL, or given) when N == Ng, otherwise an
+// interpolation I and projection P with P I = identity (true of every
+// interpolation to a finer LGL grid and the L2 projection back)
+int check_glue_ops(int N, int Ng, const double *I, const double *P,
+                   const char *side)
+{
+  const int n = N + 1, m = Ng + 1;
+  if (N == Ng)
+  {
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j)
+      {
+        const double id = i == j ? 1.0 : 0.0;
+        if ((I && std::fabs(I[i + n * j] - id) > 1e-13) ||
+            (P && std::fabs(P[i + n * j] - id) > 1e-13))
+          return fail(BFAM_GPU_EINVAL,
+                      "glue side %s has the glue order but its operators are "
+                      "not identities",
+                      side);
+      }
+    return 0;
+  }
+  if (!I || !P)
+    return fail(BFAM_GPU_EINVAL,
+                "glue side %s (order %d < glue order %d) needs both operators",
+                side, N, Ng);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j)
+    {
+      double s = 0; // (P I)(i, j): P is n x m, I is m x n
+      for (int k = 0; k < m; ++k)
+        s += P[i + n * k] * I[k + m * j];
+      if (std::fabs(s - (i == j ? 1.0 : 0.0)) > 1e-11)
+        return fail(BFAM_GPU_EINVAL,
+                    "glue side %s: projection after interpolation is not the "
+                    "identity (operators do not match orders %d and %d)",
+                    side, N, Ng);
+    }
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int bfam_gpu_pglue_create(bfam_gpu_domain_t *dm, bfam_gpu_domain_t *dp,
+                          const bfam_gpu_pglue_desc_t *desc,
+                          bfam_gpu_pglue_t **out)
+{
+  if (!out)
+    return fail(BFAM_GPU_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!dm || !dp || !desc || desc->K <= 0 || !desc->bm || !desc->bp)
+    return fail(BFAM_GPU_EINVAL, "bad glue arguments");
+  if (dm == dp)
+    return fail(BFAM_GPU_EINVAL, "a glue joins two different domains");
+  if (dm->device != dp->device || dm->dim != dp->dim || dm->flux != dp->flux)
+    return fail(BFAM_GPU_EINVAL,
+                "glued domains differ in device, dimension or flux");
+  const int Ng = desc->N_g;
+  if (Ng < std::max(dm->N, dp->N) || Ng + 1 > PGLUE_MAXQ)
+    return fail(BFAM_GPU_EINVAL,
+                "glue order %d must be >= both orders (%d, %d) and <= %d", Ng,
+                dm->N, dp->N, PGLUE_MAXQ - 1);
+  if (int rc = check_glue_ops(dm->N, Ng, desc->I_m2g, desc->P_g2m, "m"))
+    return rc;
+  if (int rc = check_glue_ops(dp->N, Ng, desc->I_p2g, desc->P_g2p, "p"))
+    return rc;
+  bfam_gpu_domain_t *d[2] = {dm, dp};
+  for (int sd = 0; sd < 2; ++sd)
+    if (int rc = host_geometry(d[sd]))
+      return rc;
+  const int32_t K = desc->K;
+  std::vector<int32_t> elem[2], slot[2];
+  std::vector<int8_t> face[2];
+  std::vector<char> seen[2];
+  for (int sd = 0; sd < 2; ++sd)
+  {
+    elem[sd].resize(K);
+    slot[sd].resize(K);
+    face[sd].resize(K);
+    seen[sd].assign(d[sd]->bslot.size(), 0);
+  }
+  for (int32_t k = 0; k < K; ++k)
+  {
+    const int32_t b[2] = {desc->bm[k], desc->bp[k]};
+    for (int sd = 0; sd < 2; ++sd)
+    {
+      const bfam_gpu_domain_t *x = d[sd];
+      if (b[sd] < 0 || b[sd] >= (int32_t)x->bslot.size() ||
+          x->bslot[b[sd]] < 0)
+        return fail(BFAM_GPU_EINVAL,
+                    "glue pair %d: entry %d of side %c is not a glued face", k,
+                    b[sd], sd ? 'p' : 'm');
+      if (seen[sd][b[sd]]++)
+        return fail(BFAM_GPU_EINVAL,
+                    "glue pair %d: entry %d of side %c is glued twice", k,
+                    b[sd], sd ? 'p' : 'm');
+      elem[sd][k] = x->bE[b[sd]];
+      face[sd][k] = x->bF[b[sd]];
+      slot[sd][k] = x->bslot[b[sd]];
+    }
+    const int f = face[0][k], ax = f >> 1;
+    if (face[1][k] != (f ^ 1))
+      return fail(BFAM_GPU_EINVAL,
+                  "glue pair %d joins faces %d and %d (need opposite faces "
+                  "of one axis)",
+                  k, f, face[1][k]);
+    // the two faces cover the same extent along the face (glue orientation
+    // 0, same size)
+    for (int a = 0; a < dm->dim; ++a)
+    {
+      if (a == ax)
+        continue;
+      const size_t i0 = 3 * (size_t)elem[0][k] + a,
+                   i1 = 3 * (size_t)elem[1][k] + a;
+      const double scale = std::max(dm->hh[i0], dp->hh[i1]);
+      if (std::fabs(dm->hx0[i0] - dp->hx0[i1]) > 1e-12 * scale ||
+          std::fabs(dm->hh[i0] - dp->hh[i1]) > 1e-12 * scale)
+        return fail(BFAM_GPU_EINVAL,
+                    "glue pair %d: the faces do not coincide along axis %d "
+                    "(hanging or shifted faces are not supported)",
+                    k, a);
+    }
+  }
+  CUDA_TRY(cudaSetDevice(dm->device));
+  bfam_gpu_pglue_t *g = new bfam_gpu_pglue_t();
+  g->d[0] = dm;
+  g->d[1] = dp;
+  g->K = K;
+  g->Ng = Ng;
+  g->flux = dm->flux;
+  g->device = dm->device;
+  g->entries[0].assign(desc->bm, desc->bm + K);
+  g->entries[1].assign(desc->bp, desc->bp + K);
+  const double *ops[2][2] = {{desc->I_m2g, desc->P_g2m},
+                             {desc->I_p2g, desc->P_g2p}};
+  int rc = 0;
+  for (int sd = 0; sd < 2 && !rc; ++sd)
+  {
+    const size_t n = (size_t)(d[sd]->N + 1) * (Ng + 1);
+    rc = pglue_upload(g, &g->elem[sd], elem[sd].data(), K);
+    if (!rc)
+      rc = pglue_upload(g, &g->face[sd], face[sd].data(), K);
+    if (!rc)
+      rc = pglue_upload(g, &g->slot[sd], slot[sd].data(), K);
+    // same order: identity, applied as a copy
+    if (!rc && d[sd]->N != Ng)
+      rc = pglue_upload(g, &g->I[sd], ops[sd][0], n);
+    if (!rc && d[sd]->N != Ng)
+      rc = pglue_upload(g, &g->P[sd], ops[sd][1], n);
+  }
+  if (rc)
+  {
+    pglue_release(g);
+    return rc;
+  }
+  *out = g;
+  return 0;
+}
+
+int bfam_gpu_pglue_free(bfam_gpu_pglue_t *g)
+{
+  pglue_release(g);
+  return 0;
+}
+
+int bfam_gpu_batch_add_pglue(bfam_gpu_batch_t *b, bfam_gpu_pglue_t *g)
+{
+  if (!b || !g)
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  int idx[2] = {-1, -1};
+  for (int sd = 0; sd < 2; ++sd)
+    for (size_t i = 0; i < b->doms.size(); ++i)
+      if (b->doms[i] == g->d[sd])
+        idx[sd] = (int)i;
+  if (idx[0] < 0 || idx[1] < 0)
+    return fail(BFAM_GPU_EINVAL, "a glued domain is not in the batch");
+  for (auto *x : b->pglues)
+    if (x == g)
+      return fail(BFAM_GPU_EINVAL, "glue added twice");
+  b->pglues.push_back(g);
+  b->pglue_dom[0].push_back(idx[0]);
+  b->pglue_dom[1].push_back(idx[1]);
   drop_graphs(b);
   return 0;
 }

@@ -565,6 +565,7 @@ static int create_domain(const bfam_gpu_volume_t *vol,
   // ---- boundary faces: self-mapped and not in the glue grid
   constexpr int32_t BOUNDARY = INT32_MIN + 1;
   std::vector<int8_t> bctype(nbr.size(), -1);
+  std::vector<int32_t> bentry(nbr.size(), -1); // boundary-list entry per face
   if (bnd && bnd->K > 0)
   {
     if (!bnd->EToE || !bnd->EToF || !bnd->type)
@@ -577,7 +578,8 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       if (e < 0 || e >= K || f < 0 || f >= NF)
         return fail(BFAM_GPU_EINVAL, "boundary face %d has bad (E, F) = (%d, %d)",
                     b, e, f);
-      if (ty != BFAM_GPU_BC_FREE_SURFACE && ty != BFAM_GPU_BC_ABSORBING)
+      if (ty != BFAM_GPU_BC_FREE_SURFACE && ty != BFAM_GPU_BC_ABSORBING &&
+          ty != BFAM_GPU_BC_GLUED)
         return fail(BFAM_GPU_EINVAL, "boundary face %d has unknown type %d", b,
                     ty);
       if (nbr[(size_t)e * NF + f] != INT32_MIN)
@@ -587,6 +589,7 @@ static int create_domain(const bfam_gpu_volume_t *vol,
                     b, e, f);
       nbr[(size_t)e * NF + f] = BOUNDARY;
       bctype[(size_t)e * NF + f] = (int8_t)ty;
+      bentry[(size_t)e * NF + f] = b;
     }
   }
   for (size_t i = 0; i < nbr.size(); ++i)
@@ -603,6 +606,13 @@ static int create_domain(const bfam_gpu_volume_t *vol,
   for (int32_t g = 0; g < Kg; ++g)
     if (glue->EToHm[g] > 0)
       mslot[g] = nslot++;
+  // then one per glued face (one piece, written by the glue between domains),
+  // in boundary-list order
+  const int32_t nbnd = bnd ? bnd->K : 0;
+  std::vector<int32_t> bslot(nbnd, -1);
+  for (int32_t b = 0; b < nbnd; ++b)
+    if (bnd->type[b] == BFAM_GPU_BC_GLUED)
+      bslot[b] = nslot++;
 
   // ---- compact descriptors read by the kernel (layout in dg_common.cuh)
   std::vector<int2> fdesc((size_t)K * NF);
@@ -618,7 +628,10 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     }
     if (nb == BOUNDARY)
     {
-      fdesc[i] = make_int2((int32_t)(i / NF), 3 | (bctype[i] << 2));
+      if (bctype[i] == BFAM_GPU_BC_GLUED)
+        fdesc[i] = make_int2(bslot[bentry[i]], 2 | (1 << 2));
+      else
+        fdesc[i] = make_int2((int32_t)(i / NF), 3 | (bctype[i] << 2));
       continue;
     }
     const int32_t g0 = -1 - nb;
@@ -661,8 +674,9 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       for (int f = 0; f < NF; ++f)
       {
         const int2 ds = fdesc[(size_t)e * NF + f];
-        if ((ds.y & 3) != 2)
-          continue;
+        if ((ds.y & 3) != 2 || ((ds.y >> 2) & 1))
+          continue; // not a hanging face (a glued face's slot is written
+                    // before the stage's element launches)
         const int32_t g0 = -1 - nbr[(size_t)e * NF + f];
         for (int p = 0; p < NPc; ++p)
         {
@@ -890,6 +904,16 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     d->hx0.assign(vol->x0, vol->x0 + 3 * (size_t)vol->K);
     d->hh.assign(vol->h, vol->h + 3 * (size_t)vol->K);
   }
+  // boundary list (glued faces are joined to other domains later)
+  d->bslot = bslot;
+  d->bE.resize(nbnd);
+  d->bF.resize(nbnd);
+  for (int32_t b = 0; b < nbnd; ++b)
+  {
+    d->bE[b] = bnd->EToE[b];
+    d->bF[b] = bnd->EToF[b];
+    d->nglued += bslot[b] >= 0;
+  }
   d->hr.assign(vol->r, vol->r + d->Nq);
   d->hw.assign(vol->w, vol->w + d->Nq);
   if (cudaMemset(d->q[0], 0, state) != cudaSuccess ||
@@ -1022,6 +1046,11 @@ int bfam_gpu_domain_rhs(bfam_gpu_domain_t *d, double *const *rhs)
 {
   if (!d || !rhs)
     return fail(BFAM_GPU_EINVAL, "NULL argument");
+  if (d->nglued)
+    return fail(BFAM_GPU_EINVAL,
+                "the domain has %d faces glued to another domain: step it "
+                "in a batch with its glue",
+                d->nglued);
   CUDA_TRY(cudaSetDevice(d->device));
   if (!d->rhs)
   {
@@ -1190,6 +1219,11 @@ int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
   if (!ts || nsteps < 0)
     return fail(BFAM_GPU_EINVAL, "bad arguments");
   bfam_gpu_domain_t *d = ts->dom;
+  if (d->nglued)
+    return fail(BFAM_GPU_EINVAL,
+                "the domain has %d faces glued to another domain: step it "
+                "in a batch with its glue",
+                d->nglued);
   CUDA_TRY(cudaSetDevice(d->device));
   // a point source or receivers need the device clock, advanced once per
   // step by the post-step kernel

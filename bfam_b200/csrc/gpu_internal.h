@@ -109,6 +109,11 @@ struct bfam_gpu_domain
   // element boxes computed on the device from quadrant data ([K][3] each;
   // null when the boxes came from the host)
   double *gx0 = nullptr, *gh = nullptr;
+  // boundary list: element, face and (glued faces) mortar slot per entry;
+  // glued faces are filled by the glue between domains
+  std::vector<int32_t> bE, bslot;
+  std::vector<int8_t> bF;
+  int nglued = 0;
   // time-dependent extras: device clock, Ricker point source, receivers
   bfam_b200::DomainClock *clock = nullptr;
   bool clock_valid = false; // device clock holds the stepper's time

@@ -124,7 +124,11 @@ typedef struct
 enum
 {
   BFAM_GPU_BC_FREE_SURFACE = 0,
-  BFAM_GPU_BC_ABSORBING = 1
+  BFAM_GPU_BC_ABSORBING = 1,
+  /* glued to a face of another domain (bfam's glue grid between two volume
+   * subdomains, e.g. of different orders): the pair is declared with
+   * bfam_gpu_pglue_create and the two domains step in one batch */
+  BFAM_GPU_BC_GLUED = 2
 };
 typedef struct
 {
@@ -335,6 +339,47 @@ int bfam_gpu_batch_free(bfam_gpu_batch_t *b);
 int bfam_gpu_batch_num_groups(const bfam_gpu_batch_t *b);
 int bfam_gpu_batch_group_info(const bfam_gpu_batch_t *b, int g, int *dim,
                               int *N, int *precision, int64_t *elements);
+
+/* ------------------------------------------------------------------------
+ * Glue between two domains, e.g. of different orders (p-nonconforming
+ * faces): bfam's glue subdomain between two volume subdomains of orders N_m
+ * and N_p, whose glue order N_g >= both (src/bfam.c:7340-7414, operators
+ * from src/bfam.c:5607-5691 with the N_m != N_p branches at 5656-5667).
+ * Each side interpolates its trace to the N_g glue grid, the upwind flux is
+ * solved there, and each side's jumps are L2-projected back to its order and
+ * lifted by its own element.  The glued faces are the entries of type
+ * BFAM_GPU_BC_GLUED in each domain's boundary list; pair k joins entry bm[k]
+ * of dm with entry bp[k] of dp: opposite faces (F and F ^ 1) of elements
+ * whose boxes meet across them with the same extent along the face, face
+ * nodes in the same tangential order (glue orientation 0).  Same-size faces
+ * only (a face that is both hanging and of another order is not supported).
+ * The coupled domains step together in one batch (bfam_gpu_batch_add_pglue)
+ * with the same time step; bfam_ts_lsrk_step and bfam_gpu_domain_rhs refuse
+ * a domain with glued faces.
+ * ---------------------------------------------------------------------- */
+typedef struct
+{
+  int32_t K;          /* glued face pairs */
+  const int32_t *bm;  /* boundary-list entry of each pair in dm */
+  const int32_t *bp;  /* boundary-list entry of each pair in dp */
+  int N_g;            /* glue order, >= both domains' orders */
+  /* glue_m->interpolation[0] / projection[0] of each side: (N_g+1) x (N+1)
+   * interpolation to the glue grid and (N+1) x (N_g+1) L2 projection from
+   * it, column-major; NULL means identity (only when N == N_g) */
+  const double *I_m2g, *P_g2m;
+  const double *I_p2g, *P_g2p;
+} bfam_gpu_pglue_desc_t;
+typedef struct bfam_gpu_pglue bfam_gpu_pglue_t;
+
+int bfam_gpu_pglue_create(bfam_gpu_domain_t *dm, bfam_gpu_domain_t *dp,
+                          const bfam_gpu_pglue_desc_t *desc,
+                          bfam_gpu_pglue_t **out);
+int bfam_gpu_pglue_free(bfam_gpu_pglue_t *g);
+/* Step the glue with the batch: one coupling launch per glue and stage,
+ * before the stage's element launches.  Both domains must be in the batch;
+ * every glued face of the batch's domains must be covered by exactly one
+ * added glue when the batch steps. */
+int bfam_gpu_batch_add_pglue(bfam_gpu_batch_t *b, bfam_gpu_pglue_t *g);
 
 /* Tile shapes compiled for an order: tile t has `threads` threads per CTA
  * (one element per CTA, one thread per node and per face node; a tile with

@@ -253,6 +253,11 @@ typedef struct
    * bc[side] (sides -x, +x, -y, +y, -z, +z): 0 free surface, 1 absorbing */
   int periodic[3];
   int bc[6];
+  /* faces glued to a subdomain of another order: index per (element, face)
+   * (-1: not glued) into the caller-supplied jumps gjump[n][6][Nfp] */
+  int *gidx;
+  int nglued;
+  double *gjump;
 } oracle_t;
 
 static int32_t owner_at(const oracle_t *o, int x, int y, int z)
@@ -334,6 +339,8 @@ void oracle_free(oracle_t *o)
   free(o->mu);
   free(o->work);
   free(o->src_W);
+  free(o->gidx);
+  free(o->gjump);
   free(o);
 }
 
@@ -450,6 +457,34 @@ void oracle_set_boundary(oracle_t *o, const int *periodic, const int *bc)
     o->periodic[a] = a < o->dim ? periodic[a] : 1;
   for (int f = 0; f < 6; ++f)
     o->bc[f] = bc[f];
+}
+
+/* Faces glued to a subdomain of another order (bfam's glue between two
+ * volume subdomains, src/bfam.c:7340-7414): this oracle lifts the jumps
+ * (T* - T-, v* - v-) that the caller computes on the glue grid and
+ * projects to this subdomain's order, J[n][6][Nfp] per glued face in list
+ * order, set before each right-hand side. */
+int oracle_set_glued(oracle_t *o, int n, const int32_t *elem, const int *face)
+{
+  free(o->gidx);
+  free(o->gjump);
+  o->gidx = malloc(sizeof(int) * (size_t)o->K * o->NF);
+  for (size_t i = 0; i < (size_t)o->K * o->NF; ++i)
+    o->gidx[i] = -1;
+  for (int k = 0; k < n; ++k)
+  {
+    if (elem[k] < 0 || elem[k] >= o->K || face[k] < 0 || face[k] >= o->NF)
+      return -1;
+    o->gidx[(size_t)elem[k] * o->NF + face[k]] = k;
+  }
+  o->nglued = n;
+  o->gjump = calloc((size_t)(n > 0 ? n : 1) * 6 * o->Nfp, sizeof(double));
+  return 0;
+}
+
+void oracle_set_glued_jumps(oracle_t *o, const double *J)
+{
+  memcpy(o->gjump, J, sizeof(double) * (size_t)o->nglued * 6 * o->Nfp);
 }
 
 /* volume node of face node q on face f */
@@ -606,6 +641,25 @@ static void face_trace(const oracle_t *o, const double *q, int32_t e, int f,
 }
 
 /* rhs of one element */
+/* every field at the face nodes of face f of element e, [NFLD][Nfp] */
+void oracle_face_trace(const oracle_t *o, const double *q, int32_t e, int f,
+                       double *tr)
+{
+  face_trace(o, q, e, f, tr);
+}
+
+/* jump terms at n points: qm, qp [n][NFLD], minus side's outward normal nrm,
+ * materials {rho, lambda, mu} of both sides -> out[n][6] (T* - T-, v* - v-) */
+void oracle_point_jumps(const oracle_t *o, int n, const double *qm,
+                        const double *qp, const double *nrm,
+                        const double *matm, const double *matp, double *out)
+{
+  for (int i = 0; i < n; ++i)
+    jumps(o, qm + (size_t)i * o->NFLD, qp + (size_t)i * o->NFLD, nrm, matm[0],
+          matm[1], matm[2], matp[0], matp[1], matp[2], out + 6 * (size_t)i,
+          out + 6 * (size_t)i + 3);
+}
+
 static void element_rhs(const oracle_t *o, const double *q, int32_t e,
                         double *rhs)
 {
@@ -681,6 +735,13 @@ static void element_rhs(const oracle_t *o, const double *q, int32_t e,
     /* finest cell just outside the face, at the lower tangential corner */
     int p[3] = {ce[0], ce[1], ce[2]};
     p[a] = side ? ce[a] + s : ce[a] - 1;
+    if (o->gidx && o->gidx[(size_t)e * o->NF + f] >= 0)
+    {
+      /* glued face: the jumps come from the glue between the subdomains */
+      memcpy(Jf, o->gjump + (size_t)o->gidx[(size_t)e * o->NF + f] * NJ * Nfp,
+             sizeof(double) * NJ * Nfp);
+      goto lift;
+    }
     if (!o->periodic[a] && (p[a] < 0 || p[a] >= o->D[a]))
     {
       /* boundary face: ghost state from the element's own trace */
@@ -878,6 +939,13 @@ static int lsrk_table(int method, double *A, double *B, double *C)
     return 5;
   }
   return -1;
+}
+
+/* LSRK coefficient tables (method 0: KC54) for callers that drive the
+ * stages themselves; returns the number of stages */
+int oracle_lsrk_coeffs(int method, double *A, double *B, double *C)
+{
+  return lsrk_table(method, A, B, C);
 }
 
 static double ricker(double t, double f0, double t0)

@@ -39,6 +39,11 @@ def lib() -> C.CDLL:
                                        C.c_int, C.c_int]
         L.oracle_set_source.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_double]
         L.oracle_set_boundary.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.oracle_set_glued.argtypes = [C.c_void_p, C.c_int, i32p, C.POINTER(C.c_int)]
+        L.oracle_set_glued_jumps.argtypes = [C.c_void_p, dp]
+        L.oracle_face_trace.argtypes = [C.c_void_p, dp, C.c_int32, C.c_int, dp]
+        L.oracle_point_jumps.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp, dp, dp]
+        L.oracle_lsrk_coeffs.argtypes = [C.c_int, dp, dp, dp]
         L.oracle_sample.argtypes = [C.c_void_p, dp, C.c_int, dp, dp]
         L.oracle_energy.restype = C.c_double
         L.oracle_energy.argtypes = [C.c_void_p, dp]
@@ -171,6 +176,150 @@ class Oracle:
     def energy(self, q: np.ndarray) -> float:
         q = np.ascontiguousarray(q, dtype=np.float64)
         return float(lib().oracle_energy(self._h, _dp(q)))
+
+    # faces glued to a subdomain of another order (see PGlueOracle)
+    def set_glued(self, elem, face) -> None:
+        e = np.ascontiguousarray(elem, dtype=np.int32)
+        f = (C.c_int * len(e))(*[int(x) for x in face])
+        if lib().oracle_set_glued(self._h, len(e), e.ctypes.data_as(i32p), f):
+            raise ValueError("bad glued face")
+        self._nglued = len(e)
+
+    def set_glued_jumps(self, J: np.ndarray) -> None:
+        J = np.ascontiguousarray(J, dtype=np.float64)
+        assert J.size == self._nglued * 6 * self.Nfp
+        lib().oracle_set_glued_jumps(self._h, _dp(J))
+
+    @property
+    def Nfp(self) -> int:
+        return (self.N + 1) ** (self.dim - 1)
+
+    @property
+    def nfields(self) -> int:
+        return 9 if self.dim == 3 else 5
+
+    def face_trace(self, q: np.ndarray, e: int, f: int) -> np.ndarray:
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        out = np.empty((self.nfields, self.Nfp))
+        lib().oracle_face_trace(self._h, _dp(q), e, f, _dp(out))
+        return out
+
+    def point_jumps(self, qm, qp, nrm, matm, matp) -> np.ndarray:
+        """(T* - T-, v* - v-) at points qm, qp [n][nfields] -> [n][6]"""
+        qm = np.ascontiguousarray(qm, dtype=np.float64)
+        qp = np.ascontiguousarray(qp, dtype=np.float64)
+        out = np.empty((len(qm), 6))
+        lib().oracle_point_jumps(self._h, len(qm), _dp(qm), _dp(qp),
+                                 _dp(np.asarray(nrm, dtype=np.float64)),
+                                 _dp(np.asarray(matm, dtype=np.float64)),
+                                 _dp(np.asarray(matp, dtype=np.float64)), _dp(out))
+        return out
+
+    def material(self, e: int):
+        return [float(a[e]) for a in self._arrs]
+
+
+def lsrk_coeffs(method: int = 0):
+    A, B, Cc = np.zeros(6), np.zeros(6), np.zeros(7)
+    ns = lib().oracle_lsrk_coeffs(method, _dp(A), _dp(B), _dp(Cc))
+    if ns < 0:
+        raise ValueError("unsupported LSRK method for the oracle")
+    return A[:ns], B[:ns], Cc[:ns + 1]
+
+
+def _lgl_np(N: int):
+    r, w, _ = lgl(N)
+    return r, w
+
+
+def glue_ops(N: int, Ng: int):
+    """The oracle's own operators between order N and the glue order Ng >= N:
+    I (Ng+1 x N+1) Lagrange interpolation at the glue's LGL nodes, and the L2
+    projection P = M_N^{-1} I^T M_g (N+1 x Ng+1) with exact mass matrices
+    (Gauss-Legendre quadrature of N + Ng + 2 points), the glue_m operators
+    of src/bfam.c:5471-5514 restated."""
+    r, _ = _lgl_np(N)
+    rg, _ = _lgl_np(Ng)
+
+    def lagrange(x, nodes):
+        L = np.ones((len(x), len(nodes)))
+        for j, xj in enumerate(nodes):
+            for m, xm in enumerate(nodes):
+                if m != j:
+                    L[:, j] *= (x - xm) / (xj - xm)
+        return L
+
+    I = lagrange(rg, r)
+    xq, wq = np.polynomial.legendre.leggauss(N + Ng + 2)
+    Ln, Lg = lagrange(xq, r), lagrange(xq, rg)
+    Mn = Ln.T @ (wq[:, None] * Ln)
+    Mgn = Ln.T @ (wq[:, None] * Lg)  # int l_N l_g = I^T M_g exactly
+    P = np.linalg.solve(Mn, Mgn)
+    return I, P
+
+
+class PGlueOracle:
+    """Two oracles (subdomains of orders Na, Nb) joined at glued face pairs
+    (ea, fa) <-> (eb, fb), opposite faces of one axis with the same extent:
+    bfam's glue grid between two volume subdomains (src/bfam.c:7340-7414).
+    Each stage both traces are interpolated to the order-Ng glue grid, the
+    upwind jumps of each side are formed there with its own outward normal
+    and material, projected back to its order and lifted by its element."""
+
+    def __init__(self, oa: Oracle, ob: Oracle, pairs, Ng: int | None = None):
+        self.o = (oa, ob)
+        self.pairs = [tuple(int(x) for x in p) for p in pairs]
+        self.Ng = Ng or max(oa.N, ob.N)
+        self.ops = (glue_ops(oa.N, self.Ng), glue_ops(ob.N, self.Ng))
+        oa.set_glued([p[0] for p in self.pairs], [p[1] for p in self.pairs])
+        ob.set_glued([p[2] for p in self.pairs], [p[3] for p in self.pairs])
+        self.dim = oa.dim
+
+    def _to_glue(self, tr, I):
+        n = I.shape[1]
+        if self.dim == 2:
+            return tr @ I.T
+        t = tr.reshape(tr.shape[0], n, n)  # [c][b][a]
+        return np.einsum("jb,ia,cba->cji", I, I, t).reshape(tr.shape[0], -1)
+
+    def _from_glue(self, J, P):
+        m = P.shape[1]
+        if self.dim == 2:
+            return J @ P.T
+        t = J.reshape(J.shape[0], m, m)
+        return np.einsum("bj,ai,cji->cba", P, P, t).reshape(J.shape[0], -1)
+
+    def rhs(self, qa, qb, nthreads: int = 0):
+        oa, ob = self.o
+        (Ia, Pa), (Ib, Pb) = self.ops
+        Ja, Jb = [], []
+        for ea, fa, eb, fb in self.pairs:
+            ga = self._to_glue(oa.face_trace(qa, ea, fa), Ia)
+            gb = self._to_glue(ob.face_trace(qb, eb, fb), Ib)
+            nrm = np.zeros(3)
+            nrm[fa // 2] = 1.0 if fa % 2 else -1.0
+            ma, mb = oa.material(ea), ob.material(eb)
+            ja = oa.point_jumps(ga.T, gb.T, nrm, ma, mb).T  # [6][glue nodes]
+            jb = ob.point_jumps(gb.T, ga.T, -nrm, mb, ma).T
+            Ja.append(self._from_glue(ja, Pa))
+            Jb.append(self._from_glue(jb, Pb))
+        oa.set_glued_jumps(np.array(Ja))
+        ob.set_glued_jumps(np.array(Jb))
+        return oa.rhs(qa, nthreads), ob.rhs(qb, nthreads)
+
+    def lsrk(self, qa, qb, dt: float, nsteps: int, nthreads: int = 0):
+        A, B, _ = lsrk_coeffs(0)
+        qa = np.array(qa, dtype=np.float64, copy=True)
+        qb = np.array(qb, dtype=np.float64, copy=True)
+        da, db = np.zeros_like(qa), np.zeros_like(qb)
+        for _ in range(nsteps):
+            for s in range(len(A)):
+                ra, rb = self.rhs(qa, qb, nthreads)
+                da = A[s] * da + dt * ra
+                db = A[s] * db + dt * rb
+                qa = qa + B[s] * da
+                qb = qb + B[s] * db
+        return qa, qb
 
 
 # --------------------------------------------------- reference-compiled ops
