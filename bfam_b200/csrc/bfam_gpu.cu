@@ -606,13 +606,17 @@ static int create_domain(const bfam_gpu_volume_t *vol,
   for (int32_t g = 0; g < Kg; ++g)
     if (glue->EToHm[g] > 0)
       mslot[g] = nslot++;
-  // then one per glued face (one piece, written by the glue between domains),
-  // in boundary-list order
+  // then, per glued face in boundary-list order, as many slots as a coarse
+  // face has pieces: the glue between domains writes the first, the others
+  // stay zero, so that the stage kernel lifts it like a coarse face
   const int32_t nbnd = bnd ? bnd->K : 0;
   std::vector<int32_t> bslot(nbnd, -1);
   for (int32_t b = 0; b < nbnd; ++b)
     if (bnd->type[b] == BFAM_GPU_BC_GLUED)
-      bslot[b] = nslot++;
+    {
+      bslot[b] = nslot;
+      nslot += NPc;
+    }
 
   // ---- compact descriptors read by the kernel (layout in dg_common.cuh)
   std::vector<int2> fdesc((size_t)K * NF);
@@ -629,7 +633,7 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     if (nb == BOUNDARY)
     {
       if (bctype[i] == BFAM_GPU_BC_GLUED)
-        fdesc[i] = make_int2(bslot[bentry[i]], 2 | (1 << 2));
+        fdesc[i] = make_int2(bslot[bentry[i]], 2);
       else
         fdesc[i] = make_int2((int32_t)(i / NF), 3 | (bctype[i] << 2));
       continue;
@@ -674,7 +678,7 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       for (int f = 0; f < NF; ++f)
       {
         const int2 ds = fdesc[(size_t)e * NF + f];
-        if ((ds.y & 3) != 2 || ((ds.y >> 2) & 1))
+        if ((ds.y & 3) != 2 || nbr[(size_t)e * NF + f] == BOUNDARY)
           continue; // not a hanging face (a glued face's slot is written
                     // before the stage's element launches)
         const int32_t g0 = -1 - nbr[(size_t)e * NF + f];
@@ -860,6 +864,13 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     TRY(upload(d, &d->fslot, fslot.data(), fslot.size()));
     TRY(dev_alloc(d, (void **)&d->mbuf,
                   sizeof(double) * (size_t)nslot * 2 * dim * Nfp));
+    // the unused pieces of glued faces stay zero
+    if (cudaMemset(d->mbuf, 0, sizeof(double) * (size_t)nslot * 2 * dim *
+                                   Nfp) != cudaSuccess)
+    {
+      release(d);
+      return fail(BFAM_GPU_ECUDA, "mortar buffer memset failed");
+    }
   }
   d->nlevels = nlevels;
   d->level_off = level_off;

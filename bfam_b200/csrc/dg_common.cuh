@@ -25,9 +25,10 @@ struct ElemData
 //   3 boundary:          a = the element, b>>2 & 3 = condition
 //                        (0 free surface, 1 absorbing)
 //   2 glue, coarse side: a = mortar buffer slot of the face's first piece
-//                        (the pieces' slots are consecutive, in glue order);
-//                        b>>2 & 1: a face glued to another domain (one
-//                        piece, written by the coupling kernel)
+//                        (the pieces' slots are consecutive, in glue order;
+//                        a face glued to another domain has its jumps in
+//                        the first, written by the coupling kernel, and
+//                        zeros in the others)
 // A fine face (kind 1 with a hanging piece) writes its projected coarse-side
 // jumps to mortar slot fslot[e][f].
 // Per-domain clock in device memory, advanced once per time step by the

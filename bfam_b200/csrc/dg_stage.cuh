@@ -398,8 +398,6 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   {
     const int f = nth_bit(coarse_mask, w / Nfp), pn = w % Nfp;
     const double *mb = d.mbuf + (size_t)desc[f].x * NJ * Nfp + pn;
-    // a face glued to another domain has one piece
-    const int npc = ((desc[f].y >> 2) & 1) ? 1 : NPC;
     CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
     for (int c = 0; c < NJ; ++c)
@@ -407,8 +405,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       double sum = 0;
 #pragma unroll
       for (int p = 0; p < NPC; ++p)
-        if (p < npc)
-          sum += mb[(p * NJ + c) * Nfp];
+        sum += mb[(p * NJ + c) * Nfp];
       J[jslot<DIM>(c)] = CT(sum);
     }
     lift_face<DIM, CT>(J, f >> 1, (f & 1) ? CT(1) : CT(-1), lfac(f >> 1), me,
