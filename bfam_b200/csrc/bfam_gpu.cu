@@ -64,6 +64,9 @@ void stage_launch(const DomainView &v, int n, const StageParams &sp,
   if (mode == MODE_STAGE)
     single_kernel<DIM, N, CT, MODE_STAGE><<<grid, S::NT, smem, stream>>>(
         v, n, sp, dop);
+  else if (mode == MODE_STAGE_NC)
+    single_kernel<DIM, N, CT, MODE_STAGE_NC><<<grid, S::NT, smem, stream>>>(
+        v, n, sp, dop);
   else
     single_kernel<DIM, N, CT, MODE_RHS><<<grid, S::NT, smem, stream>>>(
         v, n, sp, dop);
@@ -84,6 +87,8 @@ template <int DIM, int N, typename CT> cudaError_t stage_prepare(int *occ)
   cudaError_t e = allow_smem(single_kernel<DIM, N, CT, MODE_STAGE>, smem);
   if (e == cudaSuccess)
     e = allow_smem(single_kernel<DIM, N, CT, MODE_RHS>, smem);
+  if (e == cudaSuccess)
+    e = allow_smem(single_kernel<DIM, N, CT, MODE_STAGE_NC>, smem);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &occ[MODE_STAGE], single_kernel<DIM, N, CT, MODE_STAGE>, S::NT, smem);
@@ -303,7 +308,11 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double C,
     // buffer: one CTA per element, balanced by the block scheduler
     const int64_t slots = (int64_t)d->ks.occ[mode] * d->sms;
     const int grid = d->ks.nbuf == 2 && n > slots ? (int)slots : n;
-    d->ks.launch(v, n, sp, d->hops.data(), mode, grid, d->stream);
+    // the first level has no coarse-side faces (unless faces glued to
+    // another domain, which are lifted like them, sit there)
+    const int m = mode == MODE_STAGE && l == 0 && !d->nglued ? MODE_STAGE_NC
+                                                             : mode;
+    d->ks.launch(v, n, sp, d->hops.data(), m, grid, d->stream);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     CUDA_TRY(cudaGetLastError());
   }

@@ -107,10 +107,13 @@ template <int N, typename CT = double> struct DiffOp
 // LGL nodes are symmetric (r_{N-i} = -r_i); the host checks this on the glue
 // grid's operators before using it.
 
+// MODE_STAGE_NC: an LSRK stage over elements without coarse-side faces
+// (the first launch level), compiled without the coarse-face pass
 enum
 {
   MODE_STAGE = 0,
-  MODE_RHS = 1
+  MODE_RHS = 1,
+  MODE_STAGE_NC = 2
 };
 
 template <int DIM, int N> struct Shape

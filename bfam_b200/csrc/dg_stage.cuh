@@ -148,7 +148,7 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
   const int t = threadIdx.x;
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
-  const bool rd = MODE == MODE_STAGE && !sp.first_stage;
+  const bool rd = MODE != MODE_RHS && !sp.first_stage;
   const int2 *desc = d.fdesc + (size_t)e * NF;
   if constexpr (S::TMA)
   {
@@ -260,9 +260,9 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
   // the update is dq = a dq + s rhs; the right-hand-side mode uses a = 0, s = 1
-  const bool rd = MODE == MODE_STAGE && !sp.first_stage;
-  const double a = MODE == MODE_STAGE ? sp.A : 0.0;
-  const double s = MODE == MODE_STAGE ? d.dt : 1.0;
+  const bool rd = MODE != MODE_RHS && !sp.first_stage;
+  const double a = MODE != MODE_RHS ? sp.A : 0.0;
+  const double s = MODE != MODE_RHS ? d.dt : 1.0;
   const ElemData me = d.ed[e];
   const int2 *desc = d.fdesc + (size_t)e * NF;
 
@@ -394,7 +394,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   }
 
   // coarse side: the pieces' projected jumps, summed in glue order, lifted
-  for (int w = t; w < ncoarse * Nfp; w += NT)
+  for (int w = t; MODE != MODE_STAGE_NC && w < ncoarse * Nfp; w += NT)
   {
     const int f = nth_bit(coarse_mask, w / Nfp), pn = w % Nfp;
     const double *mb = d.mbuf + (size_t)desc[f].x * NJ * Nfp + pn;
@@ -453,7 +453,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
 
   // ------------------------ phase 2: volume, face contributions and update
   constexpr bool DQS = stage_dqs<DIM, N, CT>();
-  if (MODE == MODE_STAGE && rd && DQS)
+  if (MODE != MODE_RHS && rd && DQS)
   {
     if constexpr (S::TMA)
     {
@@ -510,7 +510,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         acc[c] += g * d.src.force[c];
     }
 
-    if constexpr (MODE == MODE_STAGE)
+    if constexpr (MODE != MODE_RHS)
     {
       if (rd)
       {
