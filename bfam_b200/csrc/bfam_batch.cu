@@ -297,9 +297,13 @@ struct bfam_gpu_pglue
 namespace
 {
 
+// allocation ordered on the batch's stream, complete on return
 int batch_alloc(bfam_gpu_batch_t *b, void **p, size_t bytes)
 {
-  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  use_caching_pool(b->device);
+  cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, b->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess)
   {
     cudaGetLastError();
@@ -329,10 +333,11 @@ void batch_release(bfam_gpu_batch_t *b)
     cudaEventDestroy(b->fork);
   if (b->order)
     cudaEventDestroy(b->order);
+  // after the last step on the batch's stream (the groups' streams join it)
+  for (void *p : b->allocs)
+    cudaFreeAsync(p, b->stream);
   if (b->own_stream && b->stream)
     cudaStreamDestroy(b->stream);
-  for (void *p : b->allocs)
-    cudaFree(p);
   delete b;
 }
 

@@ -193,6 +193,46 @@ namespace bfam_b200
 namespace host
 {
 
+// Domain and batch memory comes from the device's default stream-ordered
+// pool, which keeps freed blocks for reuse (release threshold: never):
+// a server that creates and frees a domain per request then neither maps
+// nor unmaps device memory, and a free does not wait for the device.
+void use_caching_pool(int device)
+{
+  static std::atomic<uint64_t> done{0};
+  if (device < 0 || device >= 64 || (done.load() >> device) & 1)
+    return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
+  {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done.fetch_or(uint64_t(1) << device);
+}
+
+// free device memory plus what the pool holds unused
+size_t free_device_bytes(int device)
+{
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+    return 0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent,
+                              &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) ==
+          cudaSuccess &&
+      reserved > used)
+    free_b += reserved - used;
+  cudaGetLastError();
+  return free_b;
+}
+
+// allocation ordered on the domain's stream, complete on return (usable
+// from any stream)
 int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes)
 {
   bytes = bytes ? bytes : 16;
@@ -200,11 +240,14 @@ int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes)
     return fail(BFAM_GPU_ENOMEM,
                 "device budget exceeded: %zu + %zu bytes > budget %zu",
                 d->bytes, bytes, d->budget);
-  cudaError_t e = cudaMalloc(p, bytes);
+  use_caching_pool(d->device);
+  cudaError_t e = cudaMallocAsync(p, bytes, d->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess)
   {
     cudaGetLastError();
-    return fail(BFAM_GPU_ENOMEM, "cudaMalloc(%zu): %s", bytes,
+    return fail(BFAM_GPU_ENOMEM, "device allocation of %zu bytes: %s", bytes,
                 cudaGetErrorString(e));
   }
   d->allocs.push_back(*p);
@@ -220,7 +263,9 @@ void dev_free(bfam_gpu_domain_t *d, void *p)
   for (size_t i = 0; i < d->allocs.size(); ++i)
     if (d->allocs[i] == p)
     {
-      cudaFree(p);
+      // ordered after the domain's work; batches make the domain's stream
+      // wait for their steps, so it is also after every batch use
+      cudaFreeAsync(p, d->stream);
       d->bytes -= d->alloc_bytes[i];
       d->allocs.erase(d->allocs.begin() + i);
       d->alloc_bytes.erase(d->alloc_bytes.begin() + i);
@@ -250,7 +295,7 @@ void release(bfam_gpu_domain_t *d)
     return;
   cudaSetDevice(d->device);
   for (void *p : d->allocs)
-    cudaFree(p);
+    cudaFreeAsync(p, d->stream);
   d->allocs.clear();
   if (d->own_stream && d->stream)
     cudaStreamDestroy(d->stream);
@@ -837,9 +882,8 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       return fail(BFAM_GPU_ECUDA, "cudaSetDevice(%d): %s", opts->device,
                   cudaGetErrorString(ce));
     }
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && !d->budget)
-      d->budget = free_b;
+    if (!d->budget)
+      d->budget = free_device_bytes(opts->device);
     ce = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
     if (ce != cudaSuccess)
     {

@@ -145,6 +145,8 @@ namespace host
 
 // device allocation counted against the domain's budget, freed with it
 int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes);
+// the device's default memory pool keeps freed blocks (once per device)
+void use_caching_pool(int device);
 // fills the host copies of the element boxes (read back from the device
 // when the domain computed them from quadrant data)
 int host_geometry(bfam_gpu_domain_t *d);
