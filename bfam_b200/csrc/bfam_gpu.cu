@@ -510,6 +510,18 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     return fail(BFAM_GPU_EINVAL, "K*Np exceeds the int32 node index range");
   const int nperm = dim == 3 ? 8 : 2;
 
+  // face-node tables: gm[f][pn] = volume node of face f's node pn, and
+  // gp[(fn * nperm + ns)][pn] the same under permutation ns
+  std::vector<int32_t> gm((size_t)NF * Nfp), gp((size_t)NF * nperm * Nfp);
+  for (int f = 0; f < NF; ++f)
+    for (int pn = 0; pn < Nfp; ++pn)
+    {
+      gm[(size_t)f * Nfp + pn] = gmask_host(dim, Nq, f, pn);
+      for (int ns = 0; ns < nperm; ++ns)
+        gp[((size_t)f * nperm + ns) * Nfp + pn] =
+            gmask_host(dim, Nq, f, face_perm_host(dim, Nq, ns, pn));
+    }
+
   // ---- vmapM must be bfam's canonical face mask layout
   const size_t nmap = (size_t)K * NF * Nfp;
   for (int32_t e = 0; e < K; ++e)
@@ -517,7 +529,7 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       for (int pn = 0; pn < Nfp; ++pn)
       {
         const size_t id = ((size_t)e * NF + f) * Nfp + pn;
-        if (vol->vmapM[id] != e * Np + gmask_host(dim, Nq, f, pn))
+        if (vol->vmapM[id] != e * Np + gm[(size_t)f * Nfp + pn])
           return fail(BFAM_GPU_EINVAL,
                       "vmapM[%zu] = %d is not element %d face %d node %d",
                       id, vol->vmapM[id], e, f, pn);
@@ -547,10 +559,11 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       for (int fn = 0; fn < NF && !found; ++fn)
         for (int ns = 0; ns < nperm && !found; ++ns)
         {
+          const int32_t *g = gp.data() + ((size_t)fn * nperm + ns) * Nfp;
+          const int32_t base = nb * Np;
           bool ok = true;
           for (int pn = 0; pn < Nfp && ok; ++pn)
-            ok = P[pn] ==
-                 nb * Np + gmask_host(dim, Nq, fn, face_perm_host(dim, Nq, ns, pn));
+            ok = P[pn] == base + g[pn];
           if (ok)
           {
             found = true;
