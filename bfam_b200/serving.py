@@ -13,8 +13,10 @@ runs continuous batching:
     `chunk` steps (persistent launches per order group, graph-replayed),
     never past the end of the shortest remaining request;
   * between chunks finished requests are retired (seismograms downloaded,
-    device memory freed) and newly admitted ones join; the batch is rebuilt
-    with each domain's current time.
+    device memory returned to the pool) and the requests admitted during
+    the last chunk join; the batch is rebuilt with each domain's current
+    time and the next chunk is queued before new arrivals are set up, so
+    that the set-up overlaps the chunk on the device.
 
 Latency of a request = completion time - arrival time, on the host clock.
 The scheduling logic talks to the device through an engine object, so that
@@ -215,20 +217,7 @@ class Server:
         for r in requests:
             if estimate_device_bytes(r.n, r.N) > self.budget:
                 raise ValueError(f"request {r.id} can never fit the budget")
-        while pending or active or joining:
-            # admission: arrived requests, in arrival order, while they fit
-            while pending and (not realtime or pending[0].arrival <= now()):
-                r = pending[0]
-                est = estimate_device_bytes(r.n, r.N)
-                if used + est > self.budget or len(active) + len(joining) >= self.max_active:
-                    break
-                pending.popleft()
-                d, dt, nbytes = self.engine.create(r)
-                r.device_bytes = nbytes
-                r.admitted = now()
-                used += max(nbytes, est)
-                joining.append((r, d, dt))
-            max_used = max(max_used, used)
+        while pending or active or joining or in_flight:
             # the chunk in flight ends: retire finished requests
             if in_flight:
                 self.engine.wait()
@@ -247,6 +236,8 @@ class Server:
                         keep.append((r, d, dt))
                 active = keep
                 in_flight = 0
+            # the next chunk goes to the device at once (with the requests
+            # admitted meanwhile); new arrivals are set up while it runs
             active += joining
             joining = []
             max_act = max(max_act, len(active))
@@ -255,7 +246,20 @@ class Server:
                 self.engine.step([d for _, d, _ in active], [dt for _, _, dt in active],
                                  [r.time for r, _, _ in active], c)
                 in_flight = c
-            elif pending:
+            # admission: arrived requests, in arrival order, while they fit
+            while pending and (not realtime or pending[0].arrival <= now()):
+                r = pending[0]
+                est = estimate_device_bytes(r.n, r.N)
+                if used + est > self.budget or len(active) + len(joining) >= self.max_active:
+                    break
+                pending.popleft()
+                d, dt, nbytes = self.engine.create(r)
+                r.device_bytes = nbytes
+                r.admitted = now()
+                used += max(nbytes, est)
+                joining.append((r, d, dt))
+            max_used = max(max_used, used)
+            if not in_flight and not joining and pending:
                 wait = pending[0].arrival - now()
                 if wait > 0 and realtime:
                     self.sleep(min(wait, 0.01))
