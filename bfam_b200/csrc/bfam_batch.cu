@@ -434,6 +434,7 @@ int issue_step(bfam_gpu_batch_t *b, int p)
       sp.C = b->C[s];
       sp.first_stage = s == 0;
       sp.flux = g.flux;
+      sp.ahead = 0;
       // levels in order: coarse elements after the fine ones across their
       // hanging faces
       for (size_t l = 0; l < g.work.size(); ++l)
@@ -521,6 +522,7 @@ int issue_step_glued(bfam_gpu_batch_t *b, int p)
       sp.C = b->C[s];
       sp.first_stage = s == 0;
       sp.flux = g.flux;
+      sp.ahead = 0;
       for (size_t l = 0; l < g.work.size(); ++l)
       {
         t.launch(g.views[par], g.work[l], (int)g.nwork_l[l], sp,

@@ -79,6 +79,10 @@ struct StageParams
   double C;        // stage time t + C dt
   int first_stage; // A == 0: dq is not read
   int flux;        // 0 upwind, 1 central
+  // one element per CTA: the CTA of work item i prefetches into L2 the
+  // element of item i + ahead (about one wave of resident CTAs later), so
+  // that its loads find L2 (0: no prefetch)
+  int ahead;
 };
 
 // Ricker wavelet (1 - 2 a) exp(-a), a = (pi f0 (t - t0))^2

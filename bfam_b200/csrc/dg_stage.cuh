@@ -222,6 +222,33 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
 
 }
 
+// L2 prefetch of everything issue_element will read of element e itself
+// (state rows, dq rows after the first stage, face descriptors, element
+// data, flux constants); one thread, no completion to wait for.
+template <int DIM, int N, int MODE>
+__device__ __forceinline__ void prefetch_element(const DomainView &d,
+                                                 const StageParams &sp, int e)
+{
+  using S = Shape<DIM, N>;
+  if constexpr (S::TMA)
+  {
+    constexpr int Np = S::Np, NF = S::NF, NFLD = S::NFLD;
+    const size_t eoff = (size_t)e * Np;
+#pragma unroll
+    for (int c = 0; c < NFLD; ++c)
+      bulk_prefetch_l2(d.qin + c * d.fs + eoff, Np * sizeof(double));
+    if (MODE != MODE_RHS && !sp.first_stage)
+    {
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        bulk_prefetch_l2(d.dq + c * d.fs + eoff, Np * sizeof(double));
+    }
+    bulk_prefetch_l2(d.fdesc + (size_t)e * NF, NF * sizeof(int2));
+    bulk_prefetch_l2(d.ed + e, sizeof(ElemData));
+    bulk_prefetch_l2(d.fcE + (size_t)e * NF, NF * sizeof(double4));
+  }
+}
+
 // Compute element e from buffer b (its loads issued by issue_element; `par`
 // is the buffer's mbarrier phase parity).
 template <int DIM, int N, int NT, int MODE, typename CT, int NBUF>
@@ -576,6 +603,11 @@ __device__ __forceinline__ void stage_loop(const Item &item, int n,
     // one element per CTA (the grid covers every item)
     issue_element<DIM, N, NT, MODE, CT, 1>(item.view(idx), sp, item.elem(idx),
                                            0);
+    // a thread of another warp than the TMA issuer prefetches a later
+    // item's element while this one's loads fly
+    const int ia = idx + sp.ahead;
+    if (sp.ahead > 0 && ia < n && threadIdx.x == (NT > 32 ? 32 : 0))
+      prefetch_element<DIM, N, MODE>(item.view(ia), sp, item.elem(ia));
     compute_element<DIM, N, NT, MODE, CT, 1>(item.view(idx), sp, dop,
                                              item.elem(idx), 0, 0);
     return;
