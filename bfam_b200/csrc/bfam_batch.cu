@@ -255,6 +255,7 @@ struct bfam_gpu_batch
     std::vector<int2 *> work;
     std::vector<int64_t> nwork_l;
     std::vector<int> grid;
+    int ahead = 0; // L2 prefetch distance of one-buffer tiles (work items)
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
   };
@@ -366,6 +367,7 @@ int choose_grid(bfam_gpu_batch_t *b, bfam_gpu_batch_t::Group &g)
   // a persistent grid for two-buffer tiles; one CTA per work item for
   // one-buffer tiles
   const bool persistent = t.NBUF == 2;
+  g.ahead = persistent ? 0 : (int)std::min<int64_t>(full, INT32_MAX);
   g.grid.resize(g.nwork_l.size());
   for (size_t l = 0; l < g.nwork_l.size(); ++l)
     g.grid[l] = (int)(persistent && g.nwork_l[l] > full ? full : g.nwork_l[l]);
@@ -434,7 +436,7 @@ int issue_step(bfam_gpu_batch_t *b, int p)
       sp.C = b->C[s];
       sp.first_stage = s == 0;
       sp.flux = g.flux;
-      sp.ahead = 0;
+      sp.ahead = g.ahead;
       // levels in order: coarse elements after the fine ones across their
       // hanging faces
       for (size_t l = 0; l < g.work.size(); ++l)
@@ -522,7 +524,7 @@ int issue_step_glued(bfam_gpu_batch_t *b, int p)
       sp.C = b->C[s];
       sp.first_stage = s == 0;
       sp.flux = g.flux;
-      sp.ahead = 0;
+      sp.ahead = g.ahead;
       for (size_t l = 0; l < g.work.size(); ++l)
       {
         t.launch(g.views[par], g.work[l], (int)g.nwork_l[l], sp,
