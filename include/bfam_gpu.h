@@ -243,7 +243,9 @@ int bfam_gpu_domain_energy_noalloc(bfam_gpu_domain_t *dom, double *energy);
 double *bfam_gpu_domain_field_device_ptr(bfam_gpu_domain_t *dom, int f);
 
 /* Stream the domain launches on (cudaStream_t passed as void*; NULL is the
- * legacy default stream). */
+ * legacy default stream).  The domain's device memory is returned to the
+ * device's memory pool in stream order on this stream when the domain is
+ * freed, so the stream must outlive the domain. */
 int bfam_gpu_domain_set_stream(bfam_gpu_domain_t *dom, void *stream);
 
 /* LSRK stepper over a domain; method numbering follows bfamo_lsrk_method_t
@@ -323,7 +325,8 @@ typedef struct bfam_gpu_batch bfam_gpu_batch_t;
 int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
                           int method, const double *t0,
                           bfam_gpu_batch_t **out);
-/* Launch on this stream (NULL: the batch's own stream). */
+/* Launch on this stream (NULL: the batch's own stream); it must outlive the
+ * batch (the batch's arrays are freed in stream order on it). */
 int bfam_gpu_batch_set_stream(bfam_gpu_batch_t *b, void *stream);
 /* Advance every domain nsteps steps, domain i with step dt[i]. */
 int bfam_gpu_batch_step(bfam_gpu_batch_t *b, const double *dt, int nsteps,
