@@ -251,3 +251,40 @@ def test_gpu_glue_checks():
     b.sync()
     b.free()
     other.free()
+
+
+@pytest.mark.gpu
+def test_gpu_glue_beside_physical_boundaries():
+    """glued x sides, absorbing bottom and free-surface top (z), hanging
+    faces inside both subdomains: one boundary list carries both kinds"""
+    rng = np.random.default_rng(11)
+    meshes = []
+    for N in (3, 5):
+        flags = (rng.random((3, 3, 3)) < 0.4).astype(np.uint8)  # [z][y][x]
+        flags[..., 0] = 0
+        flags[..., -1] = 0
+        meshes.append(bf.Mesh(3, N, (3, 3, 3), L=(0.5, 1.0, 1.0),
+                              refine_flags=flags.reshape(-1),
+                              periodic=(False, True, False)))
+    ma, mb = meshes
+    ea, eb = bf.glued_x_pairs(ma, mb)
+    pairs = np.stack([ma.EToEb[ea], ma.EToFb[ea], mb.EToEb[eb], mb.EToFb[eb]], axis=1)
+    bc = (bf.BC_GLUED, bf.BC_GLUED, 0, 0, bf.BC_ABSORBING, bf.BC_FREE_SURFACE)
+    mats = [bf.material_random(ma.K, 7), bf.material_random(mb.K, 8)]
+    qa = ma.gaussian_pulse(bf.lgl_operators(3)[0], (0.4, 0.5, 0.2), 0.2)
+    qb = mb.gaussian_pulse(bf.lgl_operators(5)[0], (0.1, 0.5, 0.8), 0.2)
+    dt = min(configs.stable_dt(ma, *mats[0], 0.5), configs.stable_dt(mb, *mats[1], 0.5))
+    da = bf.GpuDomain(ma, *mats[0], bc=bc)
+    db = bf.GpuDomain(mb, *mats[1], bc=bc)
+    da.set_fields(qa)
+    db.set_fields(qb)
+    b = bf.Batch([da, db])
+    b.add_pglue(bf.PGlue(da, db, ea, eb))
+    b.step(dt, 10)
+    b.sync()
+    po = orc.PGlueOracle(orc.Oracle.from_mesh(ma, *mats[0], bc=bc),
+                         orc.Oracle.from_mesh(mb, *mats[1], bc=bc), pairs)
+    ra, rb = po.lsrk(qa, qb, dt, 10)
+    assert relerr(da.get_fields(), ra).max() < 1e-12
+    assert relerr(db.get_fields(), rb).max() < 1e-12
+    b.free()
