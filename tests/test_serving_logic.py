@@ -107,3 +107,35 @@ def test_realtime_admission_waits_for_arrivals():
     for r in reqs:
         assert r.admitted >= r.arrival - 1e-9 and r.latency > 0
     assert stats.summary()["p99_s"] >= stats.summary()["p50_s"] > 0
+
+
+def test_next_chunk_is_queued_before_new_arrivals_are_set_up():
+    """after a chunk ends the server queues the next one at once and sets up
+    the requests that arrived meanwhile while it runs: no set-up happens
+    between a chunk's end (wait) and the next chunk's launch (step)"""
+    reqs = serving.poisson_requests(1000.0, 20, seed=5, n_range=(2, 4),
+                                    steps_range=(10, 30))
+
+    class Recorder(FakeEngine):
+        def __init__(self):
+            super().__init__()
+            self.log = []
+
+        def create(self, r):
+            self.log.append("create")
+            return super().create(r)
+
+        def step(self, doms, dts, times, chunk):
+            self.log.append("step")
+            return super().step(doms, dts, times, chunk)
+
+        def wait(self):
+            self.log.append("wait")
+
+    eng = Recorder()
+    serving.Server(eng, chunk=5).run(reqs, realtime=False)
+    for i, ev in enumerate(eng.log):
+        if ev == "wait":
+            nxt = next((x for x in eng.log[i + 1:] if x != "wait"), None)
+            assert nxt in ("step", None), eng.log[i:i + 4]
+    assert eng.log.count("create") == len(reqs)
