@@ -246,6 +246,19 @@ __device__ __forceinline__ void prefetch_element(const DomainView &d,
     bulk_prefetch_l2(d.fdesc + (size_t)e * NF, NF * sizeof(int2));
     bulk_prefetch_l2(d.ed + e, sizeof(ElemData));
     bulk_prefetch_l2(d.fcE + (size_t)e * NF, NF * sizeof(double4));
+    if constexpr (MODE != MODE_STAGE_NC)
+    {
+      // the mortar slots of its coarse faces (written by an earlier launch)
+      constexpr int NJ = S::NJ, Nfp = S::Nfp, NPC = S::NPC;
+#pragma unroll 1
+      for (int f = 0; f < NF; ++f)
+      {
+        const int2 ds = d.fdesc[(size_t)e * NF + f];
+        if ((ds.y & 3) == 2)
+          bulk_prefetch_l2(d.mbuf + (size_t)ds.x * NJ * Nfp,
+                           NPC * NJ * Nfp * sizeof(double));
+      }
+    }
   }
 }
 
