@@ -367,7 +367,7 @@ int choose_grid(bfam_gpu_batch_t *b, bfam_gpu_batch_t::Group &g)
   // a persistent grid for two-buffer tiles; one CTA per work item for
   // one-buffer tiles
   const bool persistent = t.NBUF == 2;
-  g.ahead = persistent ? 0 : (int)std::min<int64_t>(full, INT32_MAX);
+  g.ahead = persistent ? 0 : (int)std::min<int64_t>(full / 2, INT32_MAX);
   g.grid.resize(g.nwork_l.size());
   for (size_t l = 0; l < g.nwork_l.size(); ++l)
     g.grid[l] = (int)(persistent && g.nwork_l[l] > full ? full : g.nwork_l[l]);

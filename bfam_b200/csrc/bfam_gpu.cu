@@ -335,8 +335,9 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double C,
   sp.C = C;
   sp.first_stage = first;
   sp.flux = d->flux;
-  // one element per CTA: prefetch one wave of resident CTAs ahead
-  sp.ahead = d->ks.nbuf == 1 ? d->ks.occ[mode] * d->sms : 0;
+  // one element per CTA: prefetch half a wave of resident CTAs ahead (about
+  // half a CTA lifetime before the element's CTA starts)
+  sp.ahead = d->ks.nbuf == 1 ? d->ks.occ[mode] * d->sms / 2 : 0;
   DomainView v = view(d, in);
   v.dt = dt;
   // one launch per level; level l's elements after level l-1's

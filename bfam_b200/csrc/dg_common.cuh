@@ -80,8 +80,8 @@ struct StageParams
   int first_stage; // A == 0: dq is not read
   int flux;        // 0 upwind, 1 central
   // one element per CTA: the CTA of work item i prefetches into L2 the
-  // element of item i + ahead (about one wave of resident CTAs later), so
-  // that its loads find L2 (0: no prefetch)
+  // element of item i + ahead (half a wave of resident CTAs later), so that
+  // its loads find L2 (0: no prefetch)
   int ahead;
 };
 
