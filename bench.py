@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg1",
-                    choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+                    choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "next"])
     ap.add_argument("--periods", type=float, default=1.0,
                     help="cfg2: periods of the analytic plane wave")
     ap.add_argument("--rates", default="10,50,200,500",
@@ -600,6 +600,135 @@ def run_serving(args):
     return 0
 
 
+def run_next_rows(args):
+    """The rows beside the hot path, measured on the cfg1 mesh family:
+    boundary faces (a bounded brick), glue between orders (two glued halves
+    stepped in one batch, beside the same halves unglued), and element
+    geometry computed on the device from quadrant data (domain set-up
+    time).  Device-timed with CUDA events; set-up on the host clock."""
+    import time
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    import bfam_b200 as bf
+    from bfam_b200 import configs
+
+    n, N, steps = args.n, 5, args.steps
+    stream = torch.cuda.Stream(device=local)
+
+    def time_domain(dom, dt):
+        dom.set_stream(stream.cuda_stream)
+        ts = bf.LSRK(dom)
+        ts.step(dt, max(3, args.warmup), use_graph=True)
+        dom.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ts.step(dt, steps, use_graph=True)
+        e1.record(stream)
+        e1.synchronize()
+        ts.free()
+        return e0.elapsed_time(e1) / 1e3
+
+    def time_batch(b, dts):
+        b.set_stream(stream.cuda_stream)
+        b.step(dts, max(3, args.warmup))
+        b.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(dts, steps)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    out = {}
+    with ClockSampler(local) as clk:
+        # periodic and bounded cfg1-family bricks
+        res = {}
+        for name, periodic in (("periodic", (True,) * 3), ("bounded", (False,) * 3)):
+            m = bf.Mesh(3, N, (n,) * 3, refine_prob=0.3, seed=0, periodic=periodic)
+            rho, lam, mu = bf.material_random(m.K, 0)
+            q0 = m.gaussian_pulse(bf.lgl_operators(N)[0], (0.5, 0.5, 0.5), 0.05)
+            dt = configs.stable_dt(m, rho, lam, mu, 0.5)
+            bc = (bf.BC_ABSORBING,) * 5 + (bf.BC_FREE_SURFACE,)
+            d = bf.GpuDomain(m, rho, lam, mu, bc=bc, device=local)
+            d.set_fields(q0)
+            t = time_domain(d, dt)
+            res[name] = {"dof_updates_per_s": m.ndof * 5 * steps / t, "elements": m.K,
+                         "boundary_faces": int(m.Kb)}
+            d.free()
+        out["boundary"] = res
+        # glued halves (orders 3 | 5 and 5 | 5) against the same halves unglued
+        rng = np.random.default_rng(0)
+        glue = {}
+        for Na, Nb in ((5, 5), (3, 5)):
+            row = {}
+            # the same refinement for both runs; none next to the glued sides
+            flag_sets = []
+            for _ in range(2):
+                flags = (rng.random((n, n, n // 2)) < 0.3).astype(np.uint8)
+                flags[..., 0] = 0
+                flags[..., -1] = 0
+                flag_sets.append(flags)
+            for glued in (True, False):
+                meshes = []
+                for Nn, flags in zip((Na, Nb), flag_sets):
+                    per = (False, True, True) if glued else (True, True, True)
+                    meshes.append(bf.Mesh(3, Nn, (n // 2, n, n), L=(0.5, 1.0, 1.0),
+                                          refine_flags=flags.reshape(-1), periodic=per))
+                doms, dts, dofs = [], [], 0
+                for m in meshes:
+                    rho, lam, mu = bf.material_random(m.K, 1)
+                    bc = (bf.BC_GLUED, bf.BC_GLUED) + (bf.BC_FREE_SURFACE,) * 4
+                    d = bf.GpuDomain(m, rho, lam, mu, bc=bc, device=local)
+                    d.set_fields(m.gaussian_pulse(bf.lgl_operators(m.N)[0],
+                                                  (0.25, 0.5, 0.5), 0.05))
+                    doms.append(d)
+                    dts.append(configs.stable_dt(m, rho, lam, mu, 0.5))
+                    dofs += m.ndof
+                b = bf.Batch(doms)
+                if glued:
+                    g = bf.PGlue(doms[0], doms[1], *bf.glued_x_pairs(*meshes))
+                    b.add_pglue(g)
+                dt = min(dts)
+                t = time_batch(b, [dt, dt])
+                row["glued" if glued else "unglued"] = {
+                    "dof_updates_per_s": dofs * 5 * steps / t,
+                    "launches_per_step": b.launches_per_step()}
+                b.free()
+                for d in doms:
+                    d.free()
+            glue[f"N{Na}|N{Nb}"] = row
+        out["glue"] = glue
+        # domain set-up: host geometry against geometry on the device
+        m = bf.Mesh(3, N, (n,) * 3, refine_prob=0.3, seed=0)
+        rho, lam, mu = bf.material_random(m.K, 0)
+        geo = {}
+        for mode in ("host", "device"):
+            best = None
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                d = bf.GpuDomain(m, rho, lam, mu, geometry=mode, device=local)
+                d.sync()
+                t = time.perf_counter() - t0
+                best = t if best is None else min(best, t)
+                d.free()
+            geo[mode] = {"create_s": best}
+        geo["upload_bytes_per_element"] = {"host": 48, "device": 20}
+        out["geometry"] = geo
+    if rank == 0:
+        line = {"metric": "DOF-updates/s", "value": out["boundary"]["bounded"]["dof_updates_per_s"],
+                "unit": "DOF-updates/s", "n_gpus": ws, "steps": steps,
+                "warmup": max(3, args.warmup), "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"rows beside the hot path on {n}^3 N={N} p=0.3 bricks: "
+                                       "bounded brick, glued halves, device geometry"},
+                **out, "roofline": None, "cpu_baseline": None, "e2e": None,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -610,6 +739,8 @@ def main():
         return run_precision(args)
     if args.config == "cfg4":
         return run_serving(args)
+    if args.config == "next":
+        return run_next_rows(args)
     import torch
     ws, rank, local = dist_init()
     torch.cuda.set_device(local)
