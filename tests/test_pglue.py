@@ -288,3 +288,23 @@ def test_gpu_glue_beside_physical_boundaries():
     assert relerr(da.get_fields(), ra).max() < 1e-12
     assert relerr(db.get_fields(), rb).max() < 1e-12
     b.free()
+
+
+def _pw_error_2d(Na, Nb, n, T=0.05):
+    ma, mb, ea, eb, pairs = split_brick(2, Na, Nb, n, nx=(n // 2, n // 2))
+    po = orc.PGlueOracle(orc.Oracle.from_mesh(ma, 1.0, 2.0, 1.0),
+                         orc.Oracle.from_mesh(mb, 1.0, 2.0, 1.0), pairs)
+    dt0 = min(configs.stable_dt(m, 1.0, 2.0, 1.0, 0.25) for m in (ma, mb))
+    steps = int(math.ceil(T / dt0))
+    qa, qb = po.lsrk(_plane_wave(ma, 0.0, 0.0), _plane_wave(mb, 0.5, 0.0), T / steps, steps)
+    ea_, eb_ = _plane_wave(ma, 0.0, T), _plane_wave(mb, 0.5, T)
+    num = ((qa - ea_) ** 2).sum() + ((qb - eb_) ** 2).sum()
+    return math.sqrt(num / ((ea_ ** 2).sum() + (eb_ ** 2).sum()))
+
+
+def test_2d_plane_wave_through_glue_of_orders_2_and_4_converges():
+    """rate of the lower order (N + 1 = 3), and below order 2 everywhere"""
+    e1 = _pw_error_2d(2, 4, 8)
+    e2 = _pw_error_2d(2, 4, 16)
+    assert math.log2(e1 / e2) > 2.7, (e1, e2)
+    assert e2 < 0.7 * _pw_error_2d(2, 2, 16)
