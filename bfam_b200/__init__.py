@@ -176,6 +176,8 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_batch_set_tile": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "bfam_gpu_launch_count": (C.c_uint64, []),
         "bfam_gpu_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+        "bfam_gpu_record_error": (C.c_int, [C.c_int, C.c_char_p]),
+        "bfam_gpu_trim_pool": (C.c_int, [C.c_int, C.c_size_t]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -401,6 +403,14 @@ class GpuDomain:
         self.r, self.w, self.wi, self.Dr = lgl_operators(N)
         ops = mortar_operators(N, N)
         self._keep = []
+        # a mesh that carries its own operators (bfam's split: its
+        # subdomain's r, w, Dr and its glue grid's interpolation/projection)
+        # passes those instead
+        own = getattr(mesh, "interp", None) is not None
+        if own:
+            self.r = np.ascontiguousarray(mesh.r, dtype=np.float64)
+            self.w = np.ascontiguousarray(mesh.w, dtype=np.float64)
+            self.Dr = np.ascontiguousarray(mesh.Dr, dtype=np.float64)
         self.rho = np.ascontiguousarray(np.broadcast_to(rho, (mesh.K,)), dtype=np.float64)
         self.lam = np.ascontiguousarray(np.broadcast_to(lam, (mesh.K,)), dtype=np.float64)
         self.mu = np.ascontiguousarray(np.broadcast_to(mu, (mesh.K,)), dtype=np.float64)
@@ -424,10 +434,16 @@ class GpuDomain:
             glue.EToFm = mesh.EToFm.ctypes.data_as(i8p)
             glue.EToHm = mesh.EToHm.ctypes.data_as(i8p)
             # interpolation = {same, r2b, r2t}; projection = {same, cfb, cft}
-            for slot, k in enumerate((0, 3, 4)):
-                glue.interpolation[slot] = _dp(ops[k]) if k else dp()
-            for slot, k in enumerate((0, 1, 2)):
-                glue.projection[slot] = _dp(ops[k]) if k else dp()
+            if own:
+                for slot in range(3):
+                    a, b = mesh.interp[slot], mesh.proj[slot]
+                    glue.interpolation[slot] = _dp(a) if a is not None else dp()
+                    glue.projection[slot] = _dp(b) if b is not None else dp()
+            else:
+                for slot, k in enumerate((0, 3, 4)):
+                    glue.interpolation[slot] = _dp(ops[k]) if k else dp()
+                for slot, k in enumerate((0, 1, 2)):
+                    glue.projection[slot] = _dp(ops[k]) if k else dp()
         opt = Options()
         opt.flux, opt.precision = flux, precision
         opt.mem_budget_bytes, opt.device = mem_budget_bytes, device

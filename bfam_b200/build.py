@@ -7,8 +7,9 @@ Products:
   bfam_b200/libbfam_b200.so  -- CUDA kernels for sm_100a, the bfam_gpu C-ABI
                                 and the host front end (mesher, operators)
   oracle/liboracle.so        -- the CPU oracle (test infrastructure)
-  oracle/_ref/*.so           -- the reference's own setup numerics compiled
-                                from its source (only where it is present)
+  oracle/_ref/*               -- the reference compiled from its source
+                                (oracle/build_ref.sh; only when
+                                BFAM_REFERENCE_DIR is set)
 """
 from __future__ import annotations
 
@@ -81,9 +82,11 @@ def build_oracle(force: bool = False) -> Path:
              "-o", str(ORACLE_LIB), str(src), "-lm"],
             check=True,
         )
-    # the reference's own setup numerics, where its source is present (the
-    # recipe skips when it is not)
-    subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh")], check=True)
+    # the reference compiled from its own source (oracle/_ref), when
+    # BFAM_REFERENCE_DIR names the reference checkout; otherwise the files
+    # already in oracle/_ref are used as they are
+    if os.environ.get("BFAM_REFERENCE_DIR"):
+        subprocess.run(["bash", str(ROOT / "oracle" / "build_ref.sh")], check=True)
     return ORACLE_LIB
 
 

@@ -301,8 +301,7 @@ namespace
 // allocation ordered on the batch's stream, complete on return
 int batch_alloc(bfam_gpu_batch_t *b, void **p, size_t bytes)
 {
-  use_caching_pool(b->device);
-  cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, b->stream);
+  cudaError_t e = pool_alloc(p, bytes ? bytes : 16, b->device, b->stream);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess)

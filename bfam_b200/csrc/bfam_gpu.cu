@@ -167,25 +167,6 @@ int gmask_host(int dim, int Nq, int f, int pn)
   }
 }
 
-int face_perm_host(int dim, int Nq, int ns, int pn)
-{
-  const int N = Nq - 1;
-  if (dim == 2)
-    return ns ? N - pn : pn;
-  const int i = pn % Nq, j = pn / Nq, ir = N - i, jr = N - j;
-  switch (ns)
-  {
-  case 0: return i + j * Nq;
-  case 1: return j + i * Nq;
-  case 2: return ir + j * Nq;
-  case 3: return jr + i * Nq;
-  case 4: return j + ir * Nq;
-  case 5: return i + jr * Nq;
-  case 6: return jr + ir * Nq;
-  default: return ir + jr * Nq;
-  }
-}
-
 } // namespace
 
 namespace bfam_b200
@@ -193,34 +174,58 @@ namespace bfam_b200
 namespace host
 {
 
-// Domain and batch memory comes from the device's default stream-ordered
-// pool, which keeps freed blocks for reuse (release threshold: never):
-// a server that creates and frees a domain per request then neither maps
-// nor unmaps device memory, and a free does not wait for the device.
-void use_caching_pool(int device)
+// Domain and batch memory comes from a stream-ordered pool that this
+// library creates per device and owns (not the device's default pool, whose
+// settings other code in the process shares).  Freed blocks stay in the pool
+// for reuse (release threshold: never): a server that creates and frees a
+// domain per request then neither maps nor unmaps device memory, and a free
+// does not wait for the device.  What the pool holds is returned to the
+// device only when the process exits.
+cudaMemPool_t library_pool(int device)
 {
-  static std::atomic<uint64_t> done{0};
-  if (device < 0 || device >= 64 || (done.load() >> device) & 1)
-    return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  if (device < 0 || device >= 64)
+    return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!pools[device])
   {
-    uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) == cudaSuccess)
+    {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      pools[device] = pool;
+    }
+    cudaGetLastError();
   }
-  cudaGetLastError();
-  done.fetch_or(uint64_t(1) << device);
+  return pools[device];
 }
 
-// free device memory plus what the pool holds unused
+// stream-ordered allocation from the library's pool (the device's default
+// pool if the library's could not be created)
+cudaError_t pool_alloc(void **p, size_t bytes, int device, cudaStream_t stream)
+{
+  cudaMemPool_t pool = library_pool(device);
+  return pool ? cudaMallocFromPoolAsync(p, bytes, pool, stream)
+              : cudaMallocAsync(p, bytes, stream);
+}
+
+// free device memory plus what the library's pool holds unused
 size_t free_device_bytes(int device)
 {
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
     return 0;
-  cudaMemPool_t pool;
+  cudaMemPool_t pool = library_pool(device);
   uint64_t reserved = 0, used = 0;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess &&
+  if (pool &&
       cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent,
                               &reserved) == cudaSuccess &&
       cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) ==
@@ -240,8 +245,7 @@ int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes)
     return fail(BFAM_GPU_ENOMEM,
                 "device budget exceeded: %zu + %zu bytes > budget %zu",
                 d->bytes, bytes, d->budget);
-  use_caching_pool(d->device);
-  cudaError_t e = cudaMallocAsync(p, bytes, d->stream);
+  cudaError_t e = pool_alloc(p, bytes, d->device, d->stream);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess)
@@ -382,6 +386,20 @@ int bfam_gpu_last_error(char *buf, size_t len)
   return (int)g_err.size();
 }
 
+int bfam_gpu_trim_pool(int device, size_t keep_bytes)
+{
+  cudaMemPool_t pool = library_pool(device);
+  if (!pool)
+    return fail(BFAM_GPU_EINVAL, "no memory pool for device %d", device);
+  CUDA_TRY(cudaMemPoolTrimTo(pool, keep_bytes));
+  return 0;
+}
+
+int bfam_gpu_record_error(int code, const char *msg)
+{
+  return fail(code, "%s", msg ? msg : "");
+}
+
 uint64_t bfam_gpu_launch_count(void) { return g_launches.load(); }
 
 static int create_domain(const bfam_gpu_volume_t *vol,
@@ -513,17 +531,11 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     return fail(BFAM_GPU_EINVAL, "K*Np exceeds the int32 node index range");
   const int nperm = dim == 3 ? 8 : 2;
 
-  // face-node tables: gm[f][pn] = volume node of face f's node pn, and
-  // gp[(fn * nperm + ns)][pn] the same under permutation ns
-  std::vector<int32_t> gm((size_t)NF * Nfp), gp((size_t)NF * nperm * Nfp);
+  // face-node tables: gm[f][pn] = volume node of face f's node pn
+  std::vector<int32_t> gm((size_t)NF * Nfp);
   for (int f = 0; f < NF; ++f)
     for (int pn = 0; pn < Nfp; ++pn)
-    {
       gm[(size_t)f * Nfp + pn] = gmask_host(dim, Nq, f, pn);
-      for (int ns = 0; ns < nperm; ++ns)
-        gp[((size_t)f * nperm + ns) * Nfp + pn] =
-            gmask_host(dim, Nq, f, face_perm_host(dim, Nq, ns, pn));
-    }
 
   // ---- vmapM must be bfam's canonical face mask layout
   const size_t nmap = (size_t)K * NF * Nfp;
@@ -538,7 +550,12 @@ static int create_domain(const bfam_gpu_volume_t *vol,
                       id, vol->vmapM[id], e, f, pn);
       }
 
-  // ---- vmapP -> (neighbour, face, permutation) or glue face
+  // ---- vmapP -> neighbour across the opposite face, or glue face.  The
+  // element metric is diagonal (affine boxes, every tree aligned with the
+  // brick), so a face can only meet its neighbour's opposite face with the
+  // nodes in the same order (bfam's orientation 0, src/bfam.c:3630-3712); any
+  // other pairing comes from a rotated tree, which this metric cannot
+  // represent, and is refused.
   std::vector<int32_t> nbr((size_t)K * NF);
   std::vector<int8_t> nbrf((size_t)K * NF, 0);
   for (int32_t e = 0; e < K; ++e)
@@ -558,27 +575,36 @@ static int create_domain(const bfam_gpu_volume_t *vol,
         return fail(BFAM_GPU_EINVAL, "vmapP out of range at element %d face %d",
                     e, f);
       const int32_t nb = P[0] / Np;
-      bool found = false;
-      for (int fn = 0; fn < NF && !found; ++fn)
-        for (int ns = 0; ns < nperm && !found; ++ns)
+      const int fn = f ^ 1;
+      const int32_t *g = gm.data() + (size_t)fn * Nfp;
+      bool ok = true;
+      for (int pn = 0; pn < Nfp && ok; ++pn)
+        ok = P[pn] == nb * Np + g[pn];
+      if (!ok)
+      {
+        // name the pairing if vmapP is some face of nb at all
+        for (int f2 = 0; f2 < NF; ++f2)
         {
-          const int32_t *g = gp.data() + ((size_t)fn * nperm + ns) * Nfp;
-          const int32_t base = nb * Np;
-          bool ok = true;
-          for (int pn = 0; pn < Nfp && ok; ++pn)
-            ok = P[pn] == base + g[pn];
-          if (ok)
-          {
-            found = true;
-            nbr[(size_t)e * NF + f] = nb;
-            nbrf[(size_t)e * NF + f] = (int8_t)(fn + NF * ns);
-          }
+          std::vector<int32_t> want(Nfp), have(P, P + Nfp);
+          for (int pn = 0; pn < Nfp; ++pn)
+            want[pn] = nb * Np + gm[(size_t)f2 * Nfp + pn];
+          std::sort(want.begin(), want.end());
+          std::sort(have.begin(), have.end());
+          if (want == have)
+            return fail(BFAM_GPU_EUNSUPPORTED,
+                        "element %d face %d meets face %d of element %d "
+                        "%s: only aligned trees are supported (opposite "
+                        "faces, orientation 0; the element metric is "
+                        "diagonal)",
+                        e, f, f2, nb,
+                        f2 == fn ? "with permuted nodes" : "");
         }
-      if (!found)
         return fail(BFAM_GPU_EINVAL,
-                    "vmapP of element %d face %d is not a face of element %d "
-                    "under any orientation",
+                    "vmapP of element %d face %d is not a face of element %d",
                     e, f, nb);
+      }
+      nbr[(size_t)e * NF + f] = nb;
+      nbrf[(size_t)e * NF + f] = (int8_t)fn;
     }
 
   // ---- glue grid
@@ -628,6 +654,13 @@ static int create_domain(const bfam_gpu_volume_t *vol,
       if (glue->EToOp[gg] < 0 || glue->EToOp[gg] >= nperm)
         return fail(BFAM_GPU_EINVAL, "glue orientation %d out of range",
                     glue->EToOp[gg]);
+      if (glue->EToOp[gg] != 0 || glue->EToFm[pg] != (f ^ 1))
+        return fail(BFAM_GPU_EUNSUPPORTED,
+                    "glue element %d pairs face %d with face %d under "
+                    "orientation %d: only aligned trees are supported "
+                    "(opposite faces, orientation 0; the element metric is "
+                    "diagonal)",
+                    gg, f, glue->EToFm[pg], glue->EToOp[gg]);
     }
     nbr[(size_t)e * NF + f] = -1 - g;
     g += cnt;
@@ -696,8 +729,7 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     const int32_t nb = nbr[i];
     if (nb >= 0)
     {
-      const int code = nbrf[i];
-      fdesc[i] = make_int2(nb, 0 | ((code % NF) << 2) | ((code / NF) << 5));
+      fdesc[i] = make_int2(nb, 0 | (nbrf[i] << 2));
       continue;
     }
     if (nb == BOUNDARY)
@@ -713,7 +745,6 @@ static int create_domain(const bfam_gpu_volume_t *vol,
     {
       const int32_t pg = glue->EToEp[g0];
       fdesc[i] = make_int2(glue->EToEm[pg], 1 | (glue->EToFm[pg] << 2) |
-                                                (glue->EToOp[g0] << 5) |
                                                 (glue->EToHm[pg] << 8));
       if (glue->EToHm[pg] > 0)
         fslot[i] = mslot[pg];
@@ -1054,13 +1085,30 @@ int bfam_gpu_domain_set_stream(bfam_gpu_domain_t *d, void *stream)
 {
   if (!d)
     return fail(BFAM_GPU_EINVAL, "domain is NULL");
-  if (d->own_stream && d->stream)
+  CUDA_TRY(cudaSetDevice(d->device));
+  cudaStream_t next = (cudaStream_t)stream;
+  if (next != d->stream)
   {
-    cudaSetDevice(d->device);
-    cudaStreamDestroy(d->stream);
+    // work queued on the old stream (asynchronous steps, stream-ordered
+    // frees) comes before anything queued on the new one
+    cudaEvent_t ev;
+    CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, d->stream);
+    if (e == cudaSuccess)
+      e = cudaStreamWaitEvent(next, ev, 0);
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess)
+    {
+      cudaGetLastError();
+      return fail(BFAM_GPU_ECUDA, "ordering the new stream after the old: %s",
+                  cudaGetErrorString(e));
+    }
+    // a stream destroyed with work pending is released once that work ends
+    if (d->own_stream && d->stream)
+      cudaStreamDestroy(d->stream);
   }
   d->own_stream = false;
-  d->stream = (cudaStream_t)stream;
+  d->stream = next;
   return 0;
 }
 

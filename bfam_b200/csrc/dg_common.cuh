@@ -17,10 +17,10 @@ struct ElemData
 
 // Face descriptor, one per (element, face), built on the host from vmapP and
 // the glue grid.  b & 3 is the kind:
-//   0 conforming:        a = neighbour element, b>>2 & 7 = its face,
-//                        b>>5 & 7 = node permutation code
+//   0 conforming:        a = neighbour element, b>>2 & 7 = its face (the
+//                        opposite one: trees are aligned, orientation 0)
 //   1 glue, whole face:  a = partner element (same size or coarse),
-//                        b>>2 & 7 = partner face, b>>5 & 7 = glue orientation,
+//                        b>>2 & 7 = partner face,
 //                        b>>8 & 7 = partner's hanging piece (0: same size)
 //   3 boundary:          a = the element, b>>2 & 3 = condition
 //                        (0 free surface, 1 absorbing)
@@ -290,47 +290,6 @@ template <int DIM, int N> __device__ __forceinline__ int gmask(int f, int pn)
   case 3: return a + Nq * N + Nq * Nq * b;
   case 4: return a + Nq * b;
   default: return a + Nq * b + Nq * Nq * N;
-  }
-}
-
-// neighbour face-node of my face node pn under permutation code ns
-// (bfam_subdomain_dgx_buildmaps, src/bfam.c:6823-6866)
-template <int DIM, int N> __device__ __forceinline__ int face_perm(int ns, int pn)
-{
-  constexpr int Nq = N + 1;
-  if (DIM == 2)
-    return ns ? N - pn : pn;
-  const int i = pn % Nq, j = pn / Nq, ir = N - i, jr = N - j;
-  switch (ns)
-  {
-  case 0: return i + j * Nq;
-  case 1: return j + i * Nq;
-  case 2: return ir + j * Nq;
-  case 3: return jr + i * Nq;
-  case 4: return j + ir * Nq;
-  case 5: return i + jr * Nq;
-  case 6: return jr + ir * Nq;
-  default: return ir + jr * Nq;
-  }
-}
-
-// glue orientation map mapOp[o][n] (src/bfam.c:7430-7461)
-template <int DIM, int N> __device__ __forceinline__ int map_op(int o, int pn)
-{
-  constexpr int Nq = N + 1;
-  if (DIM == 2)
-    return o ? N - pn : pn;
-  const int i = pn % Nq, j = pn / Nq, ir = N - i, jr = N - j;
-  switch (o)
-  {
-  case 0: return i + j * Nq;
-  case 1: return j + i * Nq;
-  case 2: return ir + j * Nq;
-  case 3: return j + ir * Nq;
-  case 4: return jr + i * Nq;
-  case 5: return i + jr * Nq;
-  case 6: return jr + ir * Nq;
-  default: return ir + jr * Nq;
   }
 }
 

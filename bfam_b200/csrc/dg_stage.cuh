@@ -200,10 +200,9 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
       continue;
     if (k != 3) // a boundary face's ghost trace comes from the element itself
     {
-      const int nface = (ds.y >> 2) & 7;
-      const int src_n =
-          k == 0 ? gmask<DIM, N>(nface, face_perm<DIM, N>((ds.y >> 5) & 7, pn))
-                 : gmask<DIM, N>(nface, pn);
+      // the neighbour's opposite face, nodes in the same order (aligned
+      // trees: the host refuses any other pairing or orientation)
+      const int src_n = gmask<DIM, N>((ds.y >> 2) & 7, pn);
       const double *src = d.qin + (size_t)ds.x * Np + src_n;
       double *dst = pt + f * NFLD * Nfp + pn;
 #pragma unroll
@@ -307,14 +306,12 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   const int2 *desc = d.fdesc + (size_t)e * NF;
 
   int coarse_mask = 0, fine_mask = 0;
-  bool permuted = false; // a glue face whose partner nodes are permuted
 #pragma unroll
   for (int f = 0; f < NF; ++f)
   {
     const int y = desc[f].y;
     coarse_mask |= ((y & 3) == 2) << f;
     fine_mask |= ((y & 3) == 1 && ((y >> 8) & 7) != 0) << f;
-    permuted |= (y & 3) == 1 && ((y >> 5) & 7) != 0;
   }
   const int ncoarse = __popc(coarse_mask), nfine = __popc(fine_mask);
 
@@ -361,17 +358,15 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   }
 
   // flux on conforming and fine-side faces, lifted to the face node's field
-  // contributions, written in place over the node's own trace slots.  A
-  // thread reads only its own node's slots unless a glue face permutes its
-  // partner's nodes; only then are all reads finished before any write.  On
-  // a fine face the coarse side's jumps follow from the same Riemann
+  // contributions, written in place over the node's own trace slots (a
+  // thread reads only its own node's slots: partners' face nodes are in the
+  // same order on aligned trees).  On a fine face the coarse side's jumps follow from the same Riemann
   // solution (star state v*, S* n shared by both sides, coarse normal -n):
   //   coarse (T* - T-) = -(fine J_T) + [T],  coarse (v* - v-) = fine J_v - [v]
   // with [.] = coarse - fine as seen from the fine side; they go to mj in the
   // coarse piece's node order.
   {
     CT lc[NFLD];
-    int my_f = -1, my_pn = 0;
     if (t < NF * Nfp)
     {
       const int f = t / Nfp, pn = t % Nfp;
@@ -379,10 +374,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       const int k = y & 3;
       if (k != 2)
       {
-        my_f = f;
-        my_pn = pn;
         const int vm = gmask<DIM, N>(f, pn);
-        const int pp = k == 1 ? map_op<DIM, N>((y >> 5) & 7, pn) : pn;
+        const int pp = pn;
         CT dq[NTF], J[6];
         const double *x = pt + f * NFLD * Nfp;
         // boundary faces: ghost state v+ = v-, S+ = -S- (free surface) or
@@ -413,22 +406,9 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
           }
         }
         lift_face<DIM, CT>(J, f >> 1, sg, lfac(f >> 1), me, lc);
-        if (!permuted)
-        {
-#pragma unroll
-          for (int c = 0; c < NFLD; ++c)
-            pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
-        }
-      }
-    }
-    if (permuted)
-    {
-      __syncthreads();
-      if (my_f >= 0)
-      {
 #pragma unroll
         for (int c = 0; c < NFLD; ++c)
-          pt[(my_f * NFLD + c) * Nfp + my_pn] = double(lc[c]);
+          pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
       }
     }
   }

@@ -145,8 +145,10 @@ namespace host
 
 // device allocation counted against the domain's budget, freed with it
 int dev_alloc(bfam_gpu_domain_t *d, void **p, size_t bytes);
-// the device's default memory pool keeps freed blocks (once per device)
-void use_caching_pool(int device);
+// the library's own stream-ordered memory pool of a device (created once,
+// keeps freed blocks for reuse), and an allocation from it on a stream
+cudaMemPool_t library_pool(int device);
+cudaError_t pool_alloc(void **p, size_t bytes, int device, cudaStream_t stream);
 // fills the host copies of the element boxes (read back from the device
 // when the domain computed them from quadrant data)
 int host_geometry(bfam_gpu_domain_t *d);

@@ -243,10 +243,19 @@ int bfam_gpu_domain_energy_noalloc(bfam_gpu_domain_t *dom, double *energy);
 double *bfam_gpu_domain_field_device_ptr(bfam_gpu_domain_t *dom, int f);
 
 /* Stream the domain launches on (cudaStream_t passed as void*; NULL is the
- * legacy default stream).  The domain's device memory is returned to the
- * device's memory pool in stream order on this stream when the domain is
- * freed, so the stream must outlive the domain. */
+ * legacy default stream).  Work already queued on the previous stream (steps
+ * are asynchronous) completes before anything queued on the new one: the new
+ * stream waits for the old one's work, without blocking the host.  The
+ * domain's device memory is returned to the library's memory pool in stream
+ * order on this stream when the domain is freed, so the stream must outlive
+ * the domain. */
 int bfam_gpu_domain_set_stream(bfam_gpu_domain_t *dom, void *stream);
+
+/* Domains and batches allocate from a stream-ordered memory pool that the
+ * library creates per device and owns (other users of the device's default
+ * pool are unaffected).  Freed blocks stay in that pool for the next domain;
+ * this returns what it holds unused beyond keep_bytes to the device. */
+int bfam_gpu_trim_pool(int device, size_t keep_bytes);
 
 /* LSRK stepper over a domain; method numbering follows bfamo_lsrk_method_t
  * (0 KC54, 1 FE, 2 HEUN, 3 W33). */
@@ -402,6 +411,11 @@ uint64_t bfam_gpu_launch_count(void);
 /* Copy of the last error message of the calling thread (NUL-terminated,
  * truncated to len). Returns the message length. */
 int bfam_gpu_last_error(char *buf, size_t len);
+
+/* Record msg as the calling thread's last error and return code: for code
+ * layered on this C-ABI (the header-only adapter from bfam's objects,
+ * include/bfam_gpu_bfam.h) so that its failures read like the library's. */
+int bfam_gpu_record_error(int code, const char *msg);
 
 #ifdef __cplusplus
 }

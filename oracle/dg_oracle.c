@@ -268,9 +268,11 @@ static int32_t owner_at(const oracle_t *o, int x, int y, int z)
   return o->owner[x + (size_t)o->D[0] * (y + (size_t)o->D[1] * z)];
 }
 
-oracle_t *oracle_new(int dim, int N, int32_t K, const int32_t *ecoord,
-                     const int *nbase, const double *L, const double *rho,
-                     const double *lam, const double *mu, int flux)
+/* Elements are boxes of finest-level cells: ecoord[4e..4e+3] = (x, y, z,
+ * size) in cells of a brick of fine[a] cells per axis and extent L[a]. */
+oracle_t *oracle_new_ext(int dim, int N, int32_t K, const int32_t *ecoord,
+                         const int *fine, const double *L, const double *rho,
+                         const double *lam, const double *mu, int flux)
 {
   if ((dim != 2 && dim != 3) || N < 1 || N >= MAXQ - 1)
     return NULL;
@@ -290,8 +292,8 @@ oracle_t *oracle_new(int dim, int N, int32_t K, const int32_t *ecoord,
   o->ec = ecoord;
   for (int a = 0; a < 3; ++a)
   {
-    o->D[a] = a < dim ? 2 * nbase[a] : 1;
-    o->unit[a] = a < dim ? L[a] / (2.0 * nbase[a]) : 1.0;
+    o->D[a] = a < dim ? fine[a] : 1;
+    o->unit[a] = a < dim ? L[a] / fine[a] : 1.0;
   }
   o->rho = malloc(sizeof(double) * K);
   o->lam = malloc(sizeof(double) * K);
@@ -327,6 +329,17 @@ oracle_t *oracle_new(int dim, int N, int32_t K, const int32_t *ecoord,
       return NULL; /* elements do not tile the brick */
     }
   return o;
+}
+
+/* bricks refined at most once: the finest cells halve the base cells */
+oracle_t *oracle_new(int dim, int N, int32_t K, const int32_t *ecoord,
+                     const int *nbase, const double *L, const double *rho,
+                     const double *lam, const double *mu, int flux)
+{
+  int fine[3];
+  for (int a = 0; a < 3; ++a)
+    fine[a] = 2 * nbase[a];
+  return oracle_new_ext(dim, N, K, ecoord, fine, L, rho, lam, mu, flux);
 }
 
 void oracle_free(oracle_t *o)

@@ -32,6 +32,8 @@ def lib() -> C.CDLL:
         L.oracle_new.restype = C.c_void_p
         L.oracle_new.argtypes = [C.c_int, C.c_int, C.c_int32, i32p, C.POINTER(C.c_int),
                                  dp, dp, dp, dp, C.c_int]
+        L.oracle_new_ext.restype = C.c_void_p
+        L.oracle_new_ext.argtypes = L.oracle_new.argtypes
         L.oracle_free.argtypes = [C.c_void_p]
         L.oracle_rhs.argtypes = [C.c_void_p, dp, dp, C.c_int]
         L.oracle_lsrk.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, C.c_int, C.c_int]
@@ -82,16 +84,20 @@ def mortar(N: int):
 class Oracle:
     """FP64 CPU DG RHS / LSRK on a brick given by element boxes."""
 
-    def __init__(self, dim, N, ecoord, nbase, L, rho, lam, mu, flux=0):
+    def __init__(self, dim, N, ecoord, nbase, L, rho, lam, mu, flux=0, fine=None):
+        """ecoord[e] = (x, y, z, size) of element e in finest-level cells;
+        the brick has nbase base cells per axis, each halved once (fine=None),
+        or `fine` finest cells per axis (multi-level forests)."""
         self.ecoord = np.ascontiguousarray(ecoord, dtype=np.int32).reshape(-1)
         K = self.ecoord.size // 4
-        nb = (C.c_int * 3)(*[int(x) for x in list(nbase) + [1] * (3 - len(nbase))])
+        cells = [2 * int(x) for x in nbase] if fine is None else [int(x) for x in fine]
+        nb = (C.c_int * 3)(*(cells + [1] * (3 - len(cells))))
         LL = np.array(list(L) + [1.0] * (3 - len(L)), dtype=np.float64)
         self._arrs = [np.ascontiguousarray(np.broadcast_to(a, (K,)), dtype=np.float64)
                       for a in (rho, lam, mu)]
         self.K, self.dim, self.N = K, dim, N
-        h = lib().oracle_new(dim, N, K, self.ecoord.ctypes.data_as(i32p), nb, _dp(LL),
-                             *[_dp(a) for a in self._arrs], flux)
+        h = lib().oracle_new_ext(dim, N, K, self.ecoord.ctypes.data_as(i32p), nb, _dp(LL),
+                                 *[_dp(a) for a in self._arrs], flux)
         if not h:
             raise ValueError("oracle_new rejected the mesh")
         self._h = h

@@ -14,12 +14,22 @@ import bfam_b200 as bf
 INCLUDE = Path(__file__).resolve().parent.parent / "include"
 
 
+# header-only: static inline functions over the exported C-ABI, compiled by
+# the application against its own bfam.h
+ADAPTER = "bfam_gpu_bfam.h"
+
+
+def _code(h: Path) -> str:
+    text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+    return re.sub(r"//[^\n]*", "", text)
+
+
 def declared_functions():
     names = []
     for h in sorted(INCLUDE.glob("*.h")):
-        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
-        text = re.sub(r"//[^\n]*", "", text)
-        for m in re.finditer(r"\b(bfam_[A-Za-z0-9_]+)\s*\(", text):
+        if h.name == ADAPTER:
+            continue
+        for m in re.finditer(r"\b(bfam_[A-Za-z0-9_]+)\s*\(", _code(h)):
             names.append(m.group(1))
     return sorted(set(names))
 
@@ -30,6 +40,71 @@ def test_every_declared_symbol_is_exported():
     assert len(names) > 20
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_adapter_calls_only_exported_entry_points():
+    """The bfam adapter is header-only: every bfam_gpu_* / bfam_ts_lsrk_*
+    function it calls and does not define inline is exported."""
+    code = _code(INCLUDE / ADAPTER)
+    inline = set(re.findall(r"static inline \w+\s*\*?\s*(bfam_\w+)\s*\(", code))
+    called = set(re.findall(r"\b(bfam_(?:gpu|ts_lsrk)_\w+)\s*\(", code))
+    lib = C.CDLL(str(bf.LIB_PATH))
+    need = sorted(n for n in called - inline if not n.endswith("_t"))
+    assert "bfam_gpu_domain_create_from_quadrants" in need
+    missing = [n for n in need if not hasattr(lib, n)]
+    assert not missing, missing
+    assert {"bfam_gpu_domain_upload", "bfam_gpu_domain_upload_pxest",
+            "bfam_gpu_domain_download", "bfam_gpu_lsrk_init"} <= inline
+
+
+def test_rejects_rotated_tree_pairings():
+    """The element metric is diagonal (aligned trees): a face meeting its
+    neighbour's face with permuted nodes, a face meeting a non-opposite face
+    and a glue element with a non-zero orientation are refused as
+    unsupported, before any device call."""
+    m = bf.Mesh(3, 2, (3, 3, 3))
+    keep = []
+    Nfp, NF, Np = m.Nfp, m.Nfaces, m.Np
+    e, f = 4, 1
+    sl = slice((e * NF + f) * Nfp, (e * NF + f + 1) * Nfp)
+    nb = int(m.vmapP[sl][0]) // Np
+    # the same neighbour face with its nodes transposed (orientation 1)
+    perm = m.vmapP.copy()
+    nodes = perm[sl].reshape(m.Nq, m.Nq)
+    perm[sl] = nodes.T.reshape(-1)
+    v = _vol(m, keep)
+    v.vmapP = perm.ctypes.data_as(bf.i32p)
+    keep.append(perm)
+    rc, _ = _create(v)
+    assert rc == bf.BFAM_GPU_EUNSUPPORTED and "permuted" in bf.last_error()
+    # face f meeting the neighbour's face f (not f ^ 1)
+    other = m.vmapP.copy()
+    other[sl] = m.vmapM[(nb * NF + f) * Nfp:(nb * NF + f + 1) * Nfp]
+    v = _vol(m, keep)
+    v.vmapP = other.ctypes.data_as(bf.i32p)
+    keep.append(other)
+    rc, _ = _create(v)
+    assert rc == bf.BFAM_GPU_EUNSUPPORTED and "aligned trees" in bf.last_error()
+    # a glue element with orientation 3
+    mg = bf.Mesh(3, 2, (2, 2, 2), refine_prob=0.5, seed=1)
+    v = _vol(mg, keep)
+    ops = bf.mortar_operators(2, 2)
+    g = bf.GlueDesc()
+    op = mg.EToOp.copy()
+    op[0] = 3
+    keep += [op, ops]
+    g.K = mg.Kg
+    g.EToEp = mg.EToEp.ctypes.data_as(bf.i32p)
+    g.EToEm = mg.EToEm.ctypes.data_as(bf.i32p)
+    for name in ("EToHp", "EToFm", "EToHm"):
+        setattr(g, name, getattr(mg, name).ctypes.data_as(bf.i8p))
+    g.EToOp = op.ctypes.data_as(bf.i8p)
+    for s_, k in enumerate((0, 3, 4)):
+        g.interpolation[s_] = bf._dp(ops[k]) if k else bf.dp()
+    for s_, k in enumerate((0, 1, 2)):
+        g.projection[s_] = bf._dp(ops[k]) if k else bf.dp()
+    rc, _ = _create(v, g)
+    assert rc == bf.BFAM_GPU_EUNSUPPORTED and "orientation 3" in bf.last_error()
 
 
 def _vol(m, ops_keep):
@@ -60,7 +135,7 @@ def test_rejects_corrupt_vmapP():
     keep = []
     v = _vol(m, keep)
     bad = m.vmapP.copy()
-    bad[5] = bad[6]  # not a face of any element under any orientation
+    bad[5] = bad[6]  # not a face of the element
     v.vmapP = bad.ctypes.data_as(bf.i32p)
     rc, _ = _create(v)
     assert rc == -1 and "vmapP" in bf.last_error()

@@ -151,6 +151,38 @@ def test_plane_wave_converges_on_gpu():
     assert math.log2(errs[0] / errs[1]) > N + 1 - 0.5, errs
 
 
+def test_set_stream_orders_queued_steps():
+    """Steps are asynchronous on the domain's stream; after switching to
+    another stream, a read on the new stream sees the state after every
+    queued step (the new stream waits for the old one's work)."""
+    import torch
+    m, rho, lam, mu = _setup(3, 5, (4, 4, 4), 0.3, 2)
+    q0 = np.random.default_rng(2).standard_normal((m.nfields, m.K * m.Np))
+    dt = configs.stable_dt(m, rho, lam, mu, 0.4)
+    dom = bf.GpuDomain(m, rho, lam, mu)
+    dom.set_fields(q0)
+    ts = bf.LSRK(dom)
+    s2 = torch.cuda.Stream(device=0)
+    ts.step(dt, 40, use_graph=True)      # queued, not waited for
+    dom.set_stream(s2.cuda_stream)
+    got = dom.get_fields()                # ordered on the new stream
+    ref = orc.Oracle.from_mesh(m, rho, lam, mu).lsrk(q0, dt, 40)
+    assert relerr(got, ref).max() < TOL
+    ts.step(dt, 5)                         # and steps continue on it
+    got = dom.get_fields()
+    assert relerr(got, orc.Oracle.from_mesh(m, rho, lam, mu).lsrk(ref, dt, 5)).max() < TOL
+    ts.free()
+    dom.free()
+    torch.cuda.synchronize()
+
+
+def test_library_pool_trim():
+    m, rho, lam, mu = _setup(3, 3, (4, 4, 4), 0.3, 0)
+    dom = bf.GpuDomain(m, rho, lam, mu)
+    dom.free()
+    assert bf.lib().bfam_gpu_trim_pool(0, 0) == 0
+
+
 def test_memory_budget_is_enforced():
     m, rho, lam, mu = _setup(3, 3, (4, 4, 4), 0.3, 0)
     with pytest.raises(bf.BfamGpuError) as ei:
