@@ -45,7 +45,7 @@ CASES = [
     (3, (3, 3, 3), 2, 2, 3, 0.3, (1, 1, 1), 0),
     (3, (2, 2, 2), 5, 3, 2, 0.3, (1, 1, 1), 0),
     (3, (2, 3, 2), 3, 4, 2, 0.4, (0, 1, 0), 1),
-    (3, (2, 2, 2), 7, 5, 2, 0.25, (1, 1, 1), 0),
+    (3, (2, 2, 2), 7, 6, 2, 0.2, (1, 1, 1), 0),
 ]
 
 
