@@ -199,37 +199,100 @@ def replica_value(units_per_rank: float, t_max: float, ws: int) -> float:
     return units_per_rank * ws / t_max
 
 
-def cpu_baseline_sample(p, budget_s=12.0):
-    """The oracle (FP64 CPU restatement) on this host's cores: whole stages
-    (RHS + LSRK update) over the full mesh until budget_s elapses."""
-    from oracle import oracle as orc
-    o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
-    threads = orc.max_threads()
-    q = p.q0.copy()
+def _oracle_rate(o, q, dt, ndof, threads, budget_s, min_steps=1):
+    """DOF-updates/s of the oracle: whole KC54 steps until budget_s elapses."""
     t0 = time.perf_counter()
-    stages = 0
+    steps = 0
     while True:
-        q = o.lsrk(q, p.dt, 1, nthreads=threads)
-        stages += 5
-        if time.perf_counter() - t0 > budget_s:
+        q = o.lsrk(q, dt, 1, nthreads=threads)
+        steps += 1
+        if steps >= min_steps and time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    return {"value": p.ndof * stages / el, "unit": "DOF-updates/s", "cores": threads,
-            "kind": "port",
-            "sample": f"{stages // 5} KC54 step(s) = {stages} stages over the full "
-                      f"{p.name} mesh ({p.ndof} DOFs), {threads} threads, {el:.1f} s"}
+    return ndof * 5 * steps / el, steps, el
+
+
+def cpu_baseline_sample(p, budget_s=8.0):
+    """The oracle (FP64 CPU restatement) on this host's cores: whole KC54
+    steps over the full mesh with every host thread (the headline `value`),
+    one thread on the same mesh family at 8^3 base cells, and cfg0 (2D, N=4,
+    16x16, 100 steps) in full with one thread and with every thread."""
+    from bfam_b200 import configs
+    from oracle import oracle as orc
+    threads = orc.max_threads()
+    o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
+    v_all, st_all, el_all = _oracle_rate(o, p.q0.copy(), p.dt, p.ndof, threads, budget_s)
+    out = {"value": v_all, "unit": "DOF-updates/s", "cores": threads, "kind": "port",
+           "nproc": os.cpu_count(),
+           "sample": f"{st_all} KC54 step(s) over the full {p.name} mesh "
+                     f"({p.ndof} DOFs), {threads} threads, {el_all:.1f} s"}
+    if p.name in ("cfg1", "cfg2"):
+        small = configs.heterogeneous_brick(p.mesh.N, n=8, name=f"{p.name} n=8")
+        os1 = orc.Oracle.from_mesh(small.mesh, small.rho, small.lam, small.mu)
+        v1, st1, el1 = _oracle_rate(os1, small.q0.copy(), small.dt, small.ndof, 1, 4.0)
+        out["single_thread"] = {
+            "value": v1, "unit": "DOF-updates/s", "cores": 1,
+            "sample": f"{st1} KC54 step(s) over the {p.name} mesh family at 8^3 base "
+                      f"cells ({small.ndof} DOFs), 1 thread, {el1:.1f} s"}
+    c0 = configs.cfg0()
+    o0 = orc.Oracle.from_mesh(c0.mesh, c0.rho, c0.lam, c0.mu)
+    cfg0 = {}
+    for nt in (1, threads):
+        t0 = time.perf_counter()
+        o0.lsrk(c0.q0, c0.dt, c0.nsteps, nthreads=nt)
+        el = time.perf_counter() - t0
+        cfg0[f"{nt}_threads"] = {"value": c0.ndof * 5 * c0.nsteps / el,
+                                 "unit": "DOF-updates/s", "seconds": el}
+    out["cfg0_full"] = dict(cfg0, sample=f"cfg0: {c0.nsteps} KC54 steps, {c0.ndof} DOFs")
+    return out
+
+
+def reference_problem(name, n=32):
+    """cfg1/cfg2 built without the product library: the mesh by the
+    reference's own front end compiled from source (p4est brick, seeded
+    refinement, bfam_domain_pxest_split_dgx_subdomains), the material from
+    the reference's PCG32 (seed 0, stream 2: three draws per element in
+    element order), the Gaussian pulse at the reference's LGL nodes."""
+    import math
+    from types import SimpleNamespace
+    from oracle import bfam_ref as br
+    from oracle import oracle as orc
+    N = {"cfg1": 5, "cfg2": 7}[name]
+    m = br.BfamMesh(3, (n, n, n), N, seed=0, levels=1, prob=0.3)
+    u = orc.ref_pcg32(0, 2, 3 * m.K).astype(np.float64).reshape(m.K, 3) / 4294967296.0
+    rho = 1.0 + 2.0 * u[:, 0]
+    cp = 4.0 + 2.0 * u[:, 1]
+    cs = cp / (1.6 + 0.4 * u[:, 2])
+    mu = rho * cs * cs
+    lam = rho * (cp * cp - 2 * cs * cs)
+    x, y, z = m.node_coordinates()
+    pulse = np.exp(-((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2) / 0.05 ** 2)
+    q0 = np.zeros((9, m.K * m.Np))
+    q0[3:6] = -pulse
+    cpe = np.sqrt((lam + 2 * mu) / rho)
+    dt = float(0.5 * np.min(m.h[:, :3].min(axis=1) / cpe) / (N * N))
+    mesh = SimpleNamespace(dim=3, N=N, K=m.K, Kg=m.Kg, nbase=m.nbase, L=m.L,
+                           periodic=(True, True, True), ndof=m.K * m.Np * 9)
+    o = orc.Oracle(3, N, m.ecoord, m.nbase, m.L, rho, lam, mu, 0, fine=m.fine)
+    return SimpleNamespace(name=name, mesh=mesh, q0=q0, dt=dt, nsteps=200,
+                           ndof=mesh.ndof, oracle=o, meta={"refine_prob": 0.3})
 
 
 def run_reference(args):
-    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference's CPU path for this workload: the reference has no
+    elastic right-hand side, so it is the oracle's FP64 restatement on the
+    reference's own mesh (built by its compiled front end), timed on every
+    host thread; rank 0 only."""
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    p = build_problem(args.config, args.n)
     from oracle import oracle as orc
-    o = orc.Oracle.from_mesh(p.mesh, p.rho, p.lam, p.mu)
+    name = args.config if args.config in ("cfg1", "cfg2") else "cfg1"
+    p = reference_problem(name, args.n)
+    o = p.oracle
     threads = orc.max_threads()
     q = p.q0.copy()
-    # warm-up: one stage-equivalent; each timed step = one KC54 step
+    # warm-up: at most one KC54 step; each timed step = one KC54 step
     for _ in range(max(0, min(args.warmup, 1))):
         q = o.lsrk(q, p.dt, 1, nthreads=threads)
     steps = max(1, min(args.steps, 2))
@@ -245,8 +308,10 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_desc(p),
         "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{steps} KC54 step(s) over the full mesh (the reference "
-                                   "has no elastic RHS; this is the oracle's restatement)"},
+                         "nproc": os.cpu_count(),
+                         "sample": f"{steps} KC54 step(s) over the full mesh, built by the "
+                                   "reference's own front end (the reference has no "
+                                   "elastic RHS; this is the oracle's restatement)"},
         "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -820,8 +885,12 @@ def main():
         el = max_over_ranks(el, local)
         nbytes = host_np.nbytes
         e2e = {"value": p.ndof * ns * p.nsteps * ws / el, "unit": "DOF-updates/s",
-               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "step": f"one solve: upload state, {p.nsteps} LSRK steps, download state",
+               "h2d_bytes_per_step": nbytes / p.nsteps,
+               "d2h_bytes_per_step": nbytes / p.nsteps,
+               "h2d_bytes_per_solve": nbytes, "d2h_bytes_per_solve": nbytes,
+               "step": f"one LSRK step; the timed unit is one solve (upload the state, "
+                       f"{p.nsteps} steps, download the state), so the copies are "
+                       "counted per solve and per step amortised over it",
                "seconds": el}
         tsolve.free()
 
