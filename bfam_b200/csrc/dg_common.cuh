@@ -143,11 +143,17 @@ template <int DIM, int N> struct Shape
   static constexpr int NT = ((work + 31) / 32) * 32 > 1024
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
-  // CTAs per SM the register allocation is sized for (about 96 registers)
+  // CTAs per SM the register allocation is sized for (about 96 registers;
+  // 3D N=5: four CTAs of 224 threads at 72 registers, with dq read from L2)
   static constexpr int MINB_RAW = 65536 / (NT * 96);
   static constexpr int MINB = (DIM == 3 && N == 7)
                                   ? 2
-                                  : (MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW));
+                                  : (DIM == 3 && N == 5)
+                                        ? 4
+                                        : (MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW));
+  // dq read from global memory (L2) in the update instead of staged in
+  // shared memory
+  static constexpr bool DQ_L2 = DIM == 3 && N == 5;
   static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
   // shared memory regions in doubles (all even, so 16-byte aligned)
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q

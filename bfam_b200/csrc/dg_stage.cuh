@@ -57,41 +57,49 @@ __device__ __forceinline__ int nth_bit(int m, int i)
 }
 
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
-// aligned).  NBUF element buffers (state, face traces / lifted
+// aligned).  NBUF element buffers (state, dq, face traces / lifted
 // contributions, face flux constants) let the loads of the next element fly
-// while the current one is computed; the right-hand-side tile of the volume
-// pass, the mortar scratch, the 1-D operators, the mbarriers (one per buffer)
-// and the precision form's FP32 tile are single.  dq is not staged: it is
-// prefetched into L2 when the element's loads are issued and read from
-// global memory by the update.
-template <int DIM, int N, typename CT, int NBUF> struct Tile
+// while the current one is computed; the mortar scratch, the 1-D operators,
+// the mbarriers (q and dq per buffer) and the precision form's FP32 tile are
+// single.
+template <int DIM, int N, typename CT, int NBUF, bool DQS = true> struct Tile
 {
   using S = Shape<DIM, N>;
-  static constexpr int BUF = S::SM_QS + S::SM_PT + 4 * S::NF;
-  // right-hand side of the volume pass, [field][node] in CT
-  static constexpr int SM_RHS =
-      (int)((S::NFLD * S::Np * sizeof(CT) + 15) / 16 * 2);
-  static constexpr int OFF_RHS = NBUF * BUF;
-  static constexpr int OFF_MJ = OFF_RHS + SM_RHS;
+  // DQS: the element's dq rows are staged in shared memory (TMA); otherwise
+  // they are prefetched into L2 and read from global memory by the update
+  static constexpr int BUF =
+      S::SM_QS + (DQS ? S::SM_DQ : 0) + S::SM_PT + 4 * S::NF;
+  static constexpr int OFF_MJ = NBUF * BUF;
   static constexpr int OFF_OPS = OFF_MJ + S::SM_MJ;
   static constexpr int OFF_BAR = OFF_OPS + S::SM_IP;
   static constexpr int OFF_QV = OFF_BAR + 2 * NBUF;
   static constexpr bool NARROW = sizeof(CT) < sizeof(double);
   static constexpr int TOTAL = OFF_QV + (NARROW ? S::SM_QF : 0);
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(double);
-  // the mortar scratch also holds the volume pass's half of syz (3D)
-  static_assert(DIM == 2 || S::SM_MJ * sizeof(double) >= S::Np * sizeof(CT),
-                "mortar scratch too small for the syz half");
 };
 
 // CTAs per SM that the shape's register budget and NBUF buffers admit
 // (228 KB of shared memory per SM, 1 KB reserved per CTA)
-template <int DIM, int N, typename CT, int NBUF>
+template <int DIM, int N, typename CT, int NBUF, bool DQS = true>
 __host__ __device__ constexpr int resident_ctas()
 {
-  constexpr size_t bytes = Tile<DIM, N, CT, NBUF>::BYTES;
+  constexpr size_t bytes = Tile<DIM, N, CT, NBUF, DQS>::BYTES;
   constexpr int by_smem = bytes > 227 * 1024 ? 0 : (int)(233472 / (bytes + 1024));
   return Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
+}
+
+// dq staged in shared memory unless the shape reads it from L2 in the
+// update (Shape::DQ_L2: prefetched when the element's loads are issued; at
+// four or more resident CTAs per SM the coalesced loads cost fewer L1
+// wavefronts than the bulk copy into shared memory and the reads back), or
+// unless leaving it out admits more resident CTAs (3D N=7 in the precision
+// form: two CTAs instead of one)
+template <int DIM, int N, typename CT> __host__ __device__ constexpr bool stage_dqs()
+{
+  if (Shape<DIM, N>::DQ_L2)
+    return false;
+  return resident_ctas<DIM, N, CT, 1, true>() >=
+         resident_ctas<DIM, N, CT, 1, false>();
 }
 
 // Two buffers (loads of the next element overlap the current one) unless
@@ -99,8 +107,10 @@ __host__ __device__ constexpr int resident_ctas()
 // CTAs of 7 warps with one buffer, two with two).
 template <int DIM, int N, typename CT> __host__ __device__ constexpr int nbuf()
 {
-  return resident_ctas<DIM, N, CT, 2>() >= resident_ctas<DIM, N, CT, 1>() &&
-                 resident_ctas<DIM, N, CT, 2>() > 0
+  constexpr bool DQS = stage_dqs<DIM, N, CT>();
+  return resident_ctas<DIM, N, CT, 2, DQS>() >=
+                     resident_ctas<DIM, N, CT, 1, DQS>() &&
+                 resident_ctas<DIM, N, CT, 2, DQS>() > 0
              ? 2
              : 1;
 }
@@ -108,17 +118,20 @@ template <int DIM, int N, typename CT> __host__ __device__ constexpr int nbuf()
 // Element buffer b of the tile.
 template <int DIM, int N, typename CT, int NBUF> struct TileBuf
 {
-  double *qs, *pt, *fcf;
-  uint64_t *bq;
+  double *qs, *R, *pt, *fcf;
+  uint64_t *bq, *bdq;
   __device__ __forceinline__ explicit TileBuf(int b)
   {
     using S = Shape<DIM, N>;
-    using T = Tile<DIM, N, CT, NBUF>;
+    constexpr bool DQS = stage_dqs<DIM, N, CT>();
+    using T = Tile<DIM, N, CT, NBUF, DQS>;
     extern __shared__ __align__(16) double smem[];
     qs = smem + b * T::BUF;
-    pt = qs + S::SM_QS;
+    R = qs + S::SM_QS;
+    pt = R + (DQS ? S::SM_DQ : 0);
     fcf = pt + S::SM_PT;
     bq = reinterpret_cast<uint64_t *>(smem + T::OFF_BAR) + 2 * b;
+    bdq = bq + 1;
   }
 };
 
@@ -135,8 +148,8 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
   constexpr int Np = S::Np, Nfp = S::Nfp, NF = S::NF, NFLD = S::NFLD,
                 NTF = S::NTF;
   const TileBuf<DIM, N, CT, NBUF> tb(b);
-  double *qs = tb.qs, *pt = tb.pt, *fcf = tb.fcf;
-  uint64_t *bar_q = tb.bq;
+  double *qs = tb.qs, *R = tb.R, *pt = tb.pt, *fcf = tb.fcf;
+  uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
   const int t = threadIdx.x;
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
@@ -152,18 +165,33 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
       for (int c = 0; c < NFLD; ++c)
         bulk_g2s(qs + c * Np, d.qin + c * fs + eoff, Np * sizeof(double),
                  bar_q);
+      if (rd)
+      {
+        if constexpr (stage_dqs<DIM, N, CT>())
+        {
+          mbar_expect_tx(bar_dq, NFLD * Np * sizeof(double));
+#pragma unroll
+          for (int c = 0; c < NFLD; ++c)
+            bulk_g2s(R + c * Np, d.dq + c * fs + eoff, Np * sizeof(double),
+                     bar_dq);
+        }
+        else
+        {
+#pragma unroll
+          for (int c = 0; c < NFLD; ++c)
+            bulk_prefetch_l2(d.dq + c * fs + eoff, Np * sizeof(double));
+        }
+      }
     }
   }
   else
   {
     for (int w = t; w < NFLD * Np; w += NT)
+    {
       cp_async8(qs + w, d.qin + (w / Np) * fs + eoff + (w % Np));
-  }
-  // dq, read by the update: into L2 now (16-byte aligned rows only)
-  if constexpr (S::TMA)
-  {
-    if (rd && t < NFLD)
-      bulk_prefetch_l2(d.dq + t * fs + eoff, Np * sizeof(double));
+      if (stage_dqs<DIM, N, CT>() && rd)
+        cp_async8(R + w, d.dq + (w / Np) * fs + eoff + (w % Np));
+    }
   }
 
   // neighbour traces of conforming faces and coarse partners of fine-side
@@ -247,18 +275,17 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
                                                 int e, int b, unsigned par)
 {
   using S = Shape<DIM, N>;
-  using T = Tile<DIM, N, CT, NBUF>;
+  using T = Tile<DIM, N, CT, NBUF, stage_dqs<DIM, N, CT>()>;
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
                 NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
-                NTF = S::NTF, NL = S::NL;
+                NTF = S::NTF;
   static_assert(NT >= NF * Nfp, "one face-node work item per thread");
   // the dynamic shared array itself (not a pointer parameter), so that all
   // accesses stay in the shared window with 32-bit addressing
   extern __shared__ __align__(16) double smem[];
   const TileBuf<DIM, N, CT, NBUF> tb(b);
-  double *qs = tb.qs, *pt = tb.pt, *fcf = tb.fcf;
-  uint64_t *bar_q = tb.bq;
-  CT *rhs = reinterpret_cast<CT *>(smem + T::OFF_RHS);
+  double *qs = tb.qs, *R = tb.R, *pt = tb.pt, *fcf = tb.fcf;
+  uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
   double *mj = smem + T::OFF_MJ; // [DIM][NJ][Nfp] coarse-side jumps, by fine rank
   const CT *sD = reinterpret_cast<const CT *>(smem + T::OFF_OPS); // D
   const double *sPb = smem + T::OFF_OPS + 2 * Nq * Nq; // projection
@@ -449,16 +476,16 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   }
   __syncthreads();
 
-  // ---------------------------------------- phase 2: volume by lines
-  // work item (group, x-line): NF * Nfp items (3D: 6 Nq^2, 2D: 4 Nq), the
-  // face phase's count; results to the right-hand-side tile and (3D) g4's
-  // half of syz to the mortar scratch, free again here
-  CT *part = reinterpret_cast<CT *>(mj);
-  for (int w = t; w < NF * NL; w += NT)
-    volume_lines<DIM, N, CT>(qv, sD, dop, me, s, w / NL, w % NL, rhs, part);
-  __syncthreads();
-
-  // ------------------- phase 3: face contributions, source and update
+  // ------------------------ phase 2: volume, face contributions and update
+  constexpr bool DQS = stage_dqs<DIM, N, CT>();
+  if (MODE != MODE_RHS && rd && DQS)
+  {
+    if constexpr (S::TMA)
+    {
+      if (!mbar_wait(bar_dq, par))
+        atomicExch(d.err, 2);
+    }
+  }
   constexpr int NODE_ITERS = (Np + NT - 1) / NT;
 #pragma unroll 1
   for (int it = 0; it < NODE_ITERS; ++it)
@@ -468,11 +495,18 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       break;
     const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
     double acc[NFLD];
+    if constexpr (!NARROW)
+    {
+      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
+    }
+    else
+    {
+      CT rv[NFLD];
+      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
 #pragma unroll
-    for (int c = 0; c < NFLD; ++c)
-      acc[c] = double(rhs[c * Np + n]);
-    if constexpr (DIM == 3)
-      acc[8] += double(part[n]);
+      for (int c = 0; c < NFLD; ++c)
+        acc[c] = double(rv[c]);
+    }
 
     // lifted face contributions of the faces this node lies on
 #pragma unroll
@@ -507,7 +541,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       {
 #pragma unroll
         for (int c = 0; c < NFLD; ++c)
-          acc[c] += a * d.dq[c * fs + eoff + n];
+          acc[c] += a * (DQS ? R[c * Np + n] : d.dq[c * fs + eoff + n]);
       }
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
@@ -537,7 +571,7 @@ __device__ __forceinline__ void stage_loop(const Item &item, int n,
                                            const StageParams &sp,
                                            const DiffOp<N, CT> &dop)
 {
-  using T = Tile<DIM, N, CT, NBUF>;
+  using T = Tile<DIM, N, CT, NBUF, stage_dqs<DIM, N, CT>()>;
   constexpr int Nq = N + 1;
   extern __shared__ __align__(16) double smem[];
   if (threadIdx.x == 0)
@@ -646,7 +680,7 @@ __global__ void __launch_bounds__(NT, MINB)
 template <int DIM, int N, typename CT>
 __host__ __device__ constexpr size_t stage_smem_bytes()
 {
-  return Tile<DIM, N, CT, nbuf<DIM, N, CT>()>::BYTES;
+  return Tile<DIM, N, CT, nbuf<DIM, N, CT>(), stage_dqs<DIM, N, CT>()>::BYTES;
 }
 
 // resident CTAs per SM the register budget is sized for: the shape's choice,

@@ -10,262 +10,156 @@
 namespace bfam_b200
 {
 
-// NQ consecutive CT values from / to shared memory, in 16-byte pieces where
-// the alignment allows (every line and row of an element tile starts on a
-// 16-byte boundary when NQ is even).
-template <int NQ, typename CT>
-__device__ __forceinline__ void ld_line(const CT *p, CT *v)
-{
-  if constexpr (sizeof(CT) == 8 && NQ % 2 == 0)
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; m += 2)
-    {
-      const double2 x = *reinterpret_cast<const double2 *>(p + m);
-      v[m] = x.x;
-      v[m + 1] = x.y;
-    }
-  }
-  else if constexpr (sizeof(CT) == 4 && NQ % 4 == 0)
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; m += 4)
-    {
-      const float4 x = *reinterpret_cast<const float4 *>(p + m);
-      v[m] = x.x;
-      v[m + 1] = x.y;
-      v[m + 2] = x.z;
-      v[m + 3] = x.w;
-    }
-  }
-  else if constexpr (sizeof(CT) == 4 && NQ % 2 == 0)
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; m += 2)
-    {
-      const float2 x = *reinterpret_cast<const float2 *>(p + m);
-      v[m] = x.x;
-      v[m + 1] = x.y;
-    }
-  }
-  else
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; ++m)
-      v[m] = p[m];
-  }
-}
-
-template <int NQ, typename CT>
-__device__ __forceinline__ void st_line(CT *p, const CT *v)
-{
-  if constexpr (sizeof(CT) == 8 && NQ % 2 == 0)
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; m += 2)
-      *reinterpret_cast<double2 *>(p + m) = make_double2(v[m], v[m + 1]);
-  }
-  else if constexpr (sizeof(CT) == 4 && NQ % 4 == 0)
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; m += 4)
-      *reinterpret_cast<float4 *>(p + m) =
-          make_float4(v[m], v[m + 1], v[m + 2], v[m + 3]);
-  }
-  else if constexpr (sizeof(CT) == 4 && NQ % 2 == 0)
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; m += 2)
-      *reinterpret_cast<float2 *>(p + m) = make_float2(v[m], v[m + 1]);
-  }
-  else
-  {
-#pragma unroll
-    for (int m = 0; m < NQ; ++m)
-      p[m] = v[m];
-  }
-}
-
-// Volume right-hand side, s times
-//   rho dv/dt = div S,  dS/dt = lambda div(v) I + mu (grad v + grad v^T),
-// by lines: work item (g, l) takes x-line l of the element (nodes
-// i + Nq l, i = 0..N; l = j + Nq k) and derivative group g, three
-// derivatives of the tensor-product LGL operator, one along each axis
-// (2D: two), each evaluated at all Nq nodes of the line -- the
-// BFAM_KRON_IXIXA / IXAXI / AXIXI contractions of src/bfam.c:3519-3624
-// restricted to the line:
-//   along x: the line itself, D(i, m) from the parameter bank (constant
-//            operands), so every value is read once;
-//   along y: rows m of the line's k-plane, D(j, m) from shared memory;
-//   along z: rows (j, m), D(k, m).
-// The 18 derivatives of the 3D operator (2D: 8) split into 6 (2D: 4)
-// groups of one per axis, so that every item does the same work:
-//   3D  g0 (sxx,sxy,sxz) -> vx   g1 (sxy,syy,syz) -> vy  g2 (sxz,syz,szz) -> vz
-//       g3 (vx,vy,vz) -> sxx syy szz   g4 (vy,vx,vy) -> sxy, half of syz
-//       g5 (vz,vz,vx) -> sxz, the other half of syz
-//   2D  g0 (sxx,sxy) -> vx  g1 (sxy,syy) -> vy  g2 (vx,vy) -> sxx syy
-//       g3 (vy,vx) -> sxy
-// The results go to the right-hand-side tile rhs[field][node] (CT), g4's
-// half of syz to part[node] (3D), both in shared memory.  qv is the
-// element's state tile in CT, sD the column-major D(i, m) = sD[i + Nq m].
+// s times the volume right-hand side at node (i, j, k):
+//   rho dv/dt = div S,  dS/dt = lambda div(v) I + mu (grad v + grad v^T)
+// with the derivative along each axis the 1-D LGL differentiation matrix
+// applied along that axis -- the BFAM_KRON_IXIXA / IXAXI / AXIXI
+// contractions of src/bfam.c:3519-3624 evaluated at one node.  qs is the
+// element's state tile in CT, sD the column-major D(i,m) = sD[i + Nq m], both
+// in shared memory; lines along x are read with vector loads (2 doubles, or
+// 4 or 2 floats) where Nq allows.
 template <int DIM, int N, typename CT>
-__device__ __forceinline__ void volume_lines(const CT *qv, const CT *sD,
-                                             const DiffOp<N, CT> &dop,
-                                             const ElemData &me, double s,
-                                             int g, int l, CT *rhs, CT *part)
+__device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
+                                            const ElemData &me, double s, int i,
+                                            int j, int k, CT *rv)
 {
   using S = Shape<DIM, N>;
-  constexpr int Nq = S::Nq, Np = S::Np;
-  const int j = l % Nq, k = DIM == 3 ? l / Nq : 0;
-  int fx, fy, fz = 0;
-  if constexpr (DIM == 3)
-  {
-    switch (g)
-    {
-    case 0: fx = 3; fy = 6; fz = 7; break;
-    case 1: fx = 6; fy = 4; fz = 8; break;
-    case 2: fx = 7; fy = 8; fz = 5; break;
-    case 3: fx = 0; fy = 1; fz = 2; break;
-    case 4: fx = 1; fy = 0; fz = 1; break;
-    default: fx = 2; fy = 2; fz = 0; break;
-    }
-  }
-  else
-  {
-    switch (g)
-    {
-    case 0: fx = 2; fy = 4; break;
-    case 1: fx = 4; fy = 3; break;
-    case 2: fx = 0; fy = 1; break;
-    default: fx = 1; fy = 0; break;
-    }
-  }
-  CT A[Nq], B[Nq], C[Nq];
-  {
-    CT x[Nq];
-    ld_line<Nq, CT>(qv + fx * Np + Nq * l, x);
+  constexpr int Nq = S::Nq, Np = S::Np, NFLD = S::NFLD;
+  const CT lam = CT(me.lam), mu = CT(me.mu), irho = CT(me.irho);
+  const CT l2m = lam + CT(2) * mu;
 #pragma unroll
-    for (int i = 0; i < Nq; ++i)
+  for (int c = 0; c < NFLD; ++c)
+    rv[c] = CT(0);
+
+  // derivative of field c along axis ax at this node
+  auto deriv = [&](int c, int ax, const CT *Dl) {
+    CT acc = 0;
+    if (ax == 0)
     {
-      CT a = 0;
+      const CT *x = qs + c * Np + Nq * (j + Nq * k);
+      constexpr bool F4 = sizeof(CT) == 4 && Nq % 4 == 0;
+      if constexpr (F4)
+      {
+#pragma unroll
+        for (int m = 0; m < Nq; m += 4)
+        {
+          const float4 v = *reinterpret_cast<const float4 *>(x + m);
+          acc += Dl[m] * v.x;
+          acc += Dl[m + 1] * v.y;
+          acc += Dl[m + 2] * v.z;
+          acc += Dl[m + 3] * v.w;
+        }
+      }
+      else if constexpr (Nq % 2 == 0)
+      {
+        using V2 = typename std::conditional<sizeof(CT) == 4, float2,
+                                             double2>::type;
+#pragma unroll
+        for (int m = 0; m < Nq; m += 2)
+        {
+          const V2 v = *reinterpret_cast<const V2 *>(x + m);
+          acc += Dl[m] * v.x;
+          acc += Dl[m + 1] * v.y;
+        }
+      }
+      else
+      {
+#pragma unroll
+        for (int m = 0; m < Nq; ++m)
+          acc += Dl[m] * x[m];
+      }
+    }
+    else if (ax == 1)
+    {
+      const CT *x = qs + c * Np + i + Nq * Nq * k;
 #pragma unroll
       for (int m = 0; m < Nq; ++m)
-        a += dop.D[i + Nq * m] * x[m];
-      A[i] = a;
+        acc += Dl[m] * x[Nq * m];
     }
-  }
+    else
+    {
+      const CT *x = qs + c * Np + i + Nq * j;
 #pragma unroll
-  for (int i = 0; i < Nq; ++i)
-    B[i] = C[i] = CT(0);
-#pragma unroll
-  for (int m = 0; m < Nq; ++m)
-  {
-    CT r[Nq];
-    const CT dm = sD[j + Nq * m];
-    ld_line<Nq, CT>(qv + fy * Np + Nq * m + Nq * Nq * k, r);
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-      B[i] += dm * r[i];
-  }
-  if constexpr (DIM == 3)
+      for (int m = 0; m < Nq; ++m)
+        acc += Dl[m] * x[Nq * Nq * m];
+    }
+    return acc;
+  };
+
+  CT Dl[Nq];
+  // x
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
+      Dl[m] = sD[i + Nq * m];
+    const CT r = CT(s * me.rx);
+    const CT dvx = r * deriv(0, 0, Dl), dvy = r * deriv(1, 0, Dl);
+    if (DIM == 3)
     {
-      CT r[Nq];
-      const CT dm = sD[k + Nq * m];
-      ld_line<Nq, CT>(qv + fz * Np + Nq * j + Nq * Nq * m, r);
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        C[i] += dm * r[i];
-    }
-  }
-  const CT sx = CT(s * me.rx), sy = CT(s * me.ry), sz = CT(s * me.rz);
-#pragma unroll
-  for (int i = 0; i < Nq; ++i)
-  {
-    A[i] *= sx;
-    B[i] *= sy;
-    C[i] *= sz;
-  }
-  const CT irho = CT(me.irho), lam = CT(me.lam), mu = CT(me.mu);
-  const CT l2m = lam + CT(2) * mu;
-  CT o[Nq];
-  CT *line = rhs + Nq * l;
-  if constexpr (DIM == 3)
-  {
-    if (g < 3)
-    {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = irho * (A[i] + B[i] + C[i]);
-      st_line<Nq, CT>(line + g * Np, o);
-    }
-    else if (g == 3)
-    {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = l2m * A[i] + lam * (B[i] + C[i]);
-      st_line<Nq, CT>(line + 3 * Np, o);
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = l2m * B[i] + lam * (A[i] + C[i]);
-      st_line<Nq, CT>(line + 4 * Np, o);
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = l2m * C[i] + lam * (A[i] + B[i]);
-      st_line<Nq, CT>(line + 5 * Np, o);
-    }
-    else if (g == 4)
-    {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = mu * (A[i] + B[i]);
-      st_line<Nq, CT>(line + 6 * Np, o);
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = mu * C[i];
-      st_line<Nq, CT>(part + Nq * l, o);
+      const CT dvz = r * deriv(2, 0, Dl);
+      rv[3] += l2m * dvx;
+      rv[4] += lam * dvx;
+      rv[5] += lam * dvx;
+      rv[6] += mu * dvy;
+      rv[7] += mu * dvz;
+      rv[0] += irho * r * deriv(3, 0, Dl); // sxx
+      rv[1] += irho * r * deriv(6, 0, Dl); // sxy
+      rv[2] += irho * r * deriv(7, 0, Dl); // sxz
     }
     else
     {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = mu * (A[i] + C[i]);
-      st_line<Nq, CT>(line + 7 * Np, o);
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = mu * B[i];
-      st_line<Nq, CT>(line + 8 * Np, o);
+      rv[2] += l2m * dvx;
+      rv[3] += lam * dvx;
+      rv[4] += mu * dvy;
+      rv[0] += irho * r * deriv(2, 0, Dl); // sxx
+      rv[1] += irho * r * deriv(4, 0, Dl); // sxy
     }
   }
-  else
+  // y
   {
-    if (g < 2)
+#pragma unroll
+    for (int m = 0; m < Nq; ++m)
+      Dl[m] = sD[j + Nq * m];
+    const CT r = CT(s * me.ry);
+    const CT dvx = r * deriv(0, 1, Dl), dvy = r * deriv(1, 1, Dl);
+    if (DIM == 3)
     {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = irho * (A[i] + B[i]);
-      st_line<Nq, CT>(line + g * Np, o);
-    }
-    else if (g == 2)
-    {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = l2m * A[i] + lam * B[i];
-      st_line<Nq, CT>(line + 2 * Np, o);
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = lam * A[i] + l2m * B[i];
-      st_line<Nq, CT>(line + 3 * Np, o);
+      const CT dvz = r * deriv(2, 1, Dl);
+      rv[6] += mu * dvx;
+      rv[3] += lam * dvy;
+      rv[4] += l2m * dvy;
+      rv[5] += lam * dvy;
+      rv[8] += mu * dvz;
+      rv[0] += irho * r * deriv(6, 1, Dl); // sxy
+      rv[1] += irho * r * deriv(4, 1, Dl); // syy
+      rv[2] += irho * r * deriv(8, 1, Dl); // syz
     }
     else
     {
-#pragma unroll
-      for (int i = 0; i < Nq; ++i)
-        o[i] = mu * (A[i] + B[i]);
-      st_line<Nq, CT>(line + 4 * Np, o);
+      rv[4] += mu * dvx;
+      rv[2] += lam * dvy;
+      rv[3] += l2m * dvy;
+      rv[0] += irho * r * deriv(4, 1, Dl); // sxy
+      rv[1] += irho * r * deriv(3, 1, Dl); // syy
     }
+  }
+  // z
+  if (DIM == 3)
+  {
+#pragma unroll
+    for (int m = 0; m < Nq; ++m)
+      Dl[m] = sD[k + Nq * m];
+    const CT r = CT(s * me.rz);
+    const CT dvx = r * deriv(0, 2, Dl), dvy = r * deriv(1, 2, Dl),
+             dvz = r * deriv(2, 2, Dl);
+    rv[7] += mu * dvx;
+    rv[8] += mu * dvy;
+    rv[3] += lam * dvz;
+    rv[4] += lam * dvz;
+    rv[5] += l2m * dvz;
+    rv[0] += irho * r * deriv(7, 2, Dl); // sxz
+    rv[1] += irho * r * deriv(8, 2, Dl); // syz
+    rv[2] += irho * r * deriv(5, 2, Dl); // szz
   }
 }
 

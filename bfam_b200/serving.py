@@ -55,6 +55,11 @@ class Request:
     seismograms: np.ndarray | None = None
     device_bytes: int = 0
     dofs: int = 0
+    # latency breakdown, filled in by the server
+    setup_s: float = 0.0         # host set-up of its domain (engine.create)
+    joined: float | None = None  # first chunk it stepped in
+    rebuilds: int = 0            # batch rebuilds while it was active
+    chunks: int = 0              # chunks it stepped in
 
     @property
     def latency(self) -> float | None:
@@ -131,9 +136,16 @@ class GpuEngine:
         d.mesh = None
         return d, dt, d.device_bytes()
 
+    # host time spent per kind of engine call, for the latency breakdown
+    rebuilds = 0
+    rebuild_s = 0.0
+    launch_s = 0.0
+    wait_s = 0.0
+
     def step(self, doms, dts, times, chunk: int) -> None:
         from . import Batch
         key = tuple(id(d) for d in doms)
+        t0 = time.perf_counter()
         if self.batch is None or key != self.members:
             if self.batch is not None:
                 self.batch.free()
@@ -142,11 +154,18 @@ class GpuEngine:
             self.batch.set_stream(self.stream.cuda_stream)
             self._autotune.autotune(self.batch, cache=self._cache, device=self.device)
             self.members = key
+            self.rebuilds += 1
+            t1 = time.perf_counter()
+            self.rebuild_s += t1 - t0
+            t0 = t1
         self.batch.step(dts, chunk)
+        self.launch_s += time.perf_counter() - t0
 
     def wait(self) -> None:
         if self.batch is not None:
+            t0 = time.perf_counter()
             self.batch.sync()
+            self.wait_s += time.perf_counter() - t0
 
     def retire(self, d) -> np.ndarray:
         s = d.seismograms()
@@ -174,6 +193,40 @@ class ServeStats:
     chunks: int
     dof_updates: int
     timeline: list = field(default_factory=list)
+    engine_times: dict = field(default_factory=dict)
+
+    def breakdown(self) -> dict:
+        """Where the latency goes: per request the queueing (arrival to
+        admission), its host set-up, the wait for the next chunk boundary
+        (admission to its first chunk) and the service time (first chunk to
+        completion), with the batch rebuilds and chunks it sat through; p50
+        and p99 of each over the requests, and their means over the requests
+        at or above the p99 latency."""
+        done = [r for r in self.requests if r.latency is not None]
+        if not done:
+            return {}
+        comp = {
+            "queue_s": [r.admitted - r.arrival for r in done],
+            "setup_s": [r.setup_s for r in done],
+            "join_wait_s": [(r.joined if r.joined is not None else r.admitted) - r.admitted
+                            for r in done],
+            "service_s": [r.finished - (r.joined if r.joined is not None else r.admitted)
+                          for r in done],
+            "rebuilds": [r.rebuilds for r in done],
+            "chunks": [r.chunks for r in done],
+            "steps": [r.nsteps for r in done],
+            "dofs": [r.dofs for r in done],
+        }
+        lat = np.array([r.latency for r in done])
+        tail = lat >= np.percentile(lat, 99)
+        out = {}
+        for k, v in comp.items():
+            a = np.asarray(v, dtype=np.float64)
+            out[k] = {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
+                      "tail_mean": float(a[tail].mean())}
+        out["tail_latency_s"] = float(lat[tail].mean())
+        out["engine"] = dict(self.engine_times)
+        return out
 
     def summary(self) -> dict:
         lat = np.array([r.latency for r in self.requests if r.latency is not None])
@@ -187,6 +240,7 @@ class ServeStats:
             "max_active": self.max_active,
             "max_device_bytes": self.max_bytes,
             "chunks": self.chunks,
+            "latency_breakdown": self.breakdown(),
         }
 
 
@@ -226,6 +280,7 @@ class Server:
                 for r, d, dt in active:
                     r.steps_done += in_flight
                     r.time += in_flight * dt
+                    r.chunks += 1
                     dof_updates += r.dofs * 5 * in_flight
                     if r.steps_done >= r.nsteps:
                         r.seismograms = self.engine.retire(d)
@@ -238,13 +293,19 @@ class Server:
                 in_flight = 0
             # the next chunk goes to the device at once (with the requests
             # admitted meanwhile); new arrivals are set up while it runs
+            for r, _, _ in joining:
+                r.joined = now()
             active += joining
             joining = []
             max_act = max(max_act, len(active))
             if active:
                 c = min(self.chunk, min(r.nsteps - r.steps_done for r, _, _ in active))
+                rb0 = getattr(self.engine, "rebuilds", 0)
                 self.engine.step([d for _, d, _ in active], [dt for _, _, dt in active],
                                  [r.time for r, _, _ in active], c)
+                if getattr(self.engine, "rebuilds", 0) != rb0:
+                    for r, _, _ in active:
+                        r.rebuilds += 1
                 in_flight = c
             # admission: arrived requests, in arrival order, while they fit
             while pending and (not realtime or pending[0].arrival <= now()):
@@ -253,7 +314,9 @@ class Server:
                 if used + est > self.budget or len(active) + len(joining) >= self.max_active:
                     break
                 pending.popleft()
+                tc = self.clock()
                 d, dt, nbytes = self.engine.create(r)
+                r.setup_s = self.clock() - tc
                 r.device_bytes = nbytes
                 r.admitted = now()
                 used += max(nbytes, est)
@@ -264,4 +327,7 @@ class Server:
                 if wait > 0 and realtime:
                     self.sleep(min(wait, 0.01))
         self.engine.close()
-        return ServeStats(list(requests), now(), max_act, max_used, chunks, dof_updates)
+        times = {k: getattr(self.engine, k) for k in ("rebuilds", "rebuild_s", "launch_s",
+                                                      "wait_s") if hasattr(self.engine, k)}
+        return ServeStats(list(requests), now(), max_act, max_used, chunks, dof_updates,
+                          engine_times=times)
