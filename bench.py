@@ -894,6 +894,15 @@ def main():
                "seconds": el}
         tsolve.free()
 
+    # per-launch-level observability (event pair per launch, eager steps,
+    # outside the timed region)
+    dom.profile(True)
+    ts.step(p.dt, 2, use_graph=False)
+    per_level = dom.kernel_stats()
+    dom.profile(False)
+    for st in per_level:
+        st["frac_of_peak"] = st["gbs"] / peak if peak else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline_sample(p)
@@ -908,7 +917,8 @@ def main():
             "data": "synthetic",
             "config": dict(workload_desc(p), parallelism=f"replicas{ws}",
                            cuda_graph=use_graph),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "per_launch_level": per_level,
+            "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

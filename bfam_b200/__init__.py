@@ -105,6 +105,11 @@ class SourceDesc(C.Structure):
                 ("f0", C.c_double), ("t0", C.c_double)]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [("level", C.c_int), ("launches", C.c_int64), ("elements", C.c_int64),
+                ("ms", C.c_double), ("alg_bytes", C.c_double), ("gbs", C.c_double)]
+
+
 class Options(C.Structure):
     _fields_ = [("flux", C.c_int), ("precision", C.c_int),
                 ("mem_budget_bytes", C.c_size_t), ("device", C.c_int)]
@@ -178,6 +183,9 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
         "bfam_gpu_record_error": (C.c_int, [C.c_int, C.c_char_p]),
         "bfam_gpu_trim_pool": (C.c_int, [C.c_int, C.c_size_t]),
+        "bfam_gpu_domain_profile": (C.c_int, [vp, C.c_int]),
+        "bfam_gpu_domain_kernel_stats": (C.c_int, [vp, C.c_void_p, C.c_int,
+                                                   P(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -555,6 +563,22 @@ class GpuDomain:
 
     def set_stream(self, stream_ptr: int) -> None:
         _check(lib().bfam_gpu_domain_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def profile(self, enable: bool = True) -> None:
+        """per-launch event timing of the stage kernels (steps run eagerly
+        while it is on); enabling or disabling clears the totals"""
+        _check(lib().bfam_gpu_domain_profile(self._h, int(bool(enable))))
+
+    def kernel_stats(self) -> list[dict]:
+        """per launch level: launches, elements, device ms, algorithmic
+        bytes and GB/s since profiling was enabled"""
+        buf = (KernelStat * 16)()
+        n = C.c_int()
+        _check(lib().bfam_gpu_domain_kernel_stats(self._h, C.cast(buf, C.c_void_p), 16,
+                                                  C.byref(n)))
+        return [{"level": s.level, "launches": int(s.launches), "elements": int(s.elements),
+                 "ms": s.ms, "alg_bytes": s.alg_bytes, "gbs": s.gbs}
+                for s in buf[:min(n.value, 16)]]
 
     def set_source(self, x, force, f0: float, t0: float) -> None:
         """Ricker point force f(t) F at x (bfam_gpu_domain_set_source)."""

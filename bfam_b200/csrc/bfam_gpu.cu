@@ -10,6 +10,8 @@
 #include "dg_stage.cuh"
 #include "gpu_internal.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -298,6 +300,13 @@ void release(bfam_gpu_domain_t *d)
   if (!d)
     return;
   cudaSetDevice(d->device);
+  for (auto &pl : d->prof_pending)
+  {
+    cudaEventDestroy(pl.t0);
+    cudaEventDestroy(pl.t1);
+  }
+  for (cudaEvent_t ev : d->prof_free)
+    cudaEventDestroy(ev);
   for (void *p : d->allocs)
     cudaFreeAsync(p, d->stream);
   d->allocs.clear();
@@ -364,10 +373,62 @@ int launch_stage(bfam_gpu_domain_t *d, int in, double A, double B, double C,
     // another domain, which are lifted like them, sit there)
     const int m = mode == MODE_STAGE && l == 0 && !d->nglued ? MODE_STAGE_NC
                                                              : mode;
+    bfam_gpu_domain::ProfLaunch pl{};
+    if (d->prof)
+    {
+      for (cudaEvent_t *ev : {&pl.t0, &pl.t1})
+      {
+        if (d->prof_free.empty())
+          CUDA_TRY(cudaEventCreate(ev));
+        else
+        {
+          *ev = d->prof_free.back();
+          d->prof_free.pop_back();
+        }
+      }
+      // algorithmic bytes: q read and the new q written, dq written, and
+      // after the first stage dq read (right-hand side: q read, rhs written)
+      const double per_dof = mode == MODE_RHS ? 16.0 : (first ? 24.0 : 32.0);
+      pl.level = l;
+      pl.elements = n;
+      pl.bytes = per_dof * (double)n * d->Np * d->NFLD;
+      CUDA_TRY(cudaEventRecord(pl.t0, d->stream));
+    }
     d->ks.launch(v, n, sp, d->hops.data(), m, grid, d->stream);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     CUDA_TRY(cudaGetLastError());
+    if (d->prof)
+    {
+      CUDA_TRY(cudaEventRecord(pl.t1, d->stream));
+      d->prof_pending.push_back(pl);
+    }
   }
+  return 0;
+}
+
+// Move the finished launches' times into the per-level totals.
+int prof_drain(bfam_gpu_domain_t *d)
+{
+  for (auto &pl : d->prof_pending)
+  {
+    CUDA_TRY(cudaEventSynchronize(pl.t1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, pl.t0, pl.t1));
+    if ((int)d->prof_ms.size() <= pl.level)
+    {
+      d->prof_ms.resize(pl.level + 1, 0.0);
+      d->prof_bytes.resize(pl.level + 1, 0.0);
+      d->prof_launches.resize(pl.level + 1, 0);
+      d->prof_elements.resize(pl.level + 1, 0);
+    }
+    d->prof_ms[pl.level] += ms;
+    d->prof_bytes[pl.level] += pl.bytes;
+    d->prof_launches[pl.level] += 1;
+    d->prof_elements[pl.level] += pl.elements;
+    d->prof_free.push_back(pl.t0);
+    d->prof_free.push_back(pl.t1);
+  }
+  d->prof_pending.clear();
   return 0;
 }
 
@@ -384,6 +445,46 @@ int bfam_gpu_last_error(char *buf, size_t len)
     buf[len - 1] = 0;
   }
   return (int)g_err.size();
+}
+
+int bfam_gpu_domain_profile(bfam_gpu_domain_t *d, int enable)
+{
+  if (!d)
+    return fail(BFAM_GPU_EINVAL, "domain is NULL");
+  CUDA_TRY(cudaSetDevice(d->device));
+  int rc = prof_drain(d);
+  if (rc)
+    return rc;
+  d->prof = enable != 0;
+  d->prof_ms.clear();
+  d->prof_bytes.clear();
+  d->prof_launches.clear();
+  d->prof_elements.clear();
+  return 0;
+}
+
+int bfam_gpu_domain_kernel_stats(bfam_gpu_domain_t *d,
+                                 bfam_gpu_kernel_stat_t *out, int max_levels,
+                                 int *nlevels)
+{
+  if (!d || !nlevels || (max_levels > 0 && !out))
+    return fail(BFAM_GPU_EINVAL, "NULL argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  int rc = prof_drain(d);
+  if (rc)
+    return rc;
+  const int n = (int)d->prof_ms.size();
+  *nlevels = n;
+  for (int l = 0; l < n && l < max_levels; ++l)
+  {
+    out[l].level = l;
+    out[l].launches = d->prof_launches[l];
+    out[l].elements = d->prof_elements[l];
+    out[l].ms = d->prof_ms[l];
+    out[l].alg_bytes = d->prof_bytes[l];
+    out[l].gbs = d->prof_ms[l] > 0 ? d->prof_bytes[l] / (d->prof_ms[l] * 1e6) : 0;
+  }
+  return 0;
 }
 
 int bfam_gpu_trim_pool(int device, size_t keep_bytes)
@@ -1365,16 +1466,29 @@ int bfam_ts_lsrk_step(bfam_ts_lsrk_t *ts, double dt, int nsteps, int use_graph)
   // one step starting from state buffer c0
   auto issue = [&](int c0) -> int {
     int in = c0;
+    static const char *const stage_name[] = {"lsrk stage 0", "lsrk stage 1",
+                                             "lsrk stage 2", "lsrk stage 3",
+                                             "lsrk stage 4", "lsrk stage 5"};
     for (int s = 0; s < ts->ns; ++s, in ^= 1)
     {
+      nvtxRangePushA(stage_name[s < 6 ? s : 5]);
       int rc = launch_stage(d, in, ts->A[s], ts->B[s], ts->C[s], dt, s == 0,
                             MODE_STAGE);
+      nvtxRangePop();
       if (rc)
         return rc;
     }
     return post ? launch_post(d, in, dt) : 0;
   };
   const int per_step = ts->ns * d->nlevels + (post ? 1 : 0);
+  // per-launch timing needs eager launches
+  if (d->prof)
+    use_graph = 0;
+  struct NvtxRange
+  {
+    NvtxRange() { nvtxRangePushA("bfam_ts_lsrk_step"); }
+    ~NvtxRange() { nvtxRangePop(); }
+  } nvtx_range;
   for (int st = 0; st < nsteps; ++st)
   {
     const int c0 = d->cur;

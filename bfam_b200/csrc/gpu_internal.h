@@ -124,6 +124,20 @@ struct bfam_gpu_domain
   double *recv_w = nullptr;
   double *seis = nullptr;
   unsigned extras_gen = 0;   // bumped when the source or receivers change
+  // opt-in per-launch timing (bfam_gpu_domain_profile): an event pair
+  // around every stage launch, drained into per-level totals
+  bool prof = false;
+  struct ProfLaunch
+  {
+    cudaEvent_t t0, t1;
+    int level;
+    double bytes; // algorithmic bytes of the launch
+    int64_t elements;
+  };
+  std::vector<ProfLaunch> prof_pending;
+  std::vector<cudaEvent_t> prof_free;
+  std::vector<double> prof_ms, prof_bytes;
+  std::vector<int64_t> prof_launches, prof_elements;
 };
 
 struct bfam_ts_lsrk

@@ -251,6 +251,33 @@ double *bfam_gpu_domain_field_device_ptr(bfam_gpu_domain_t *dom, int f);
  * the domain. */
 int bfam_gpu_domain_set_stream(bfam_gpu_domain_t *dom, void *stream);
 
+/* Per-launch timing, the counterpart of the reference's KERNEL_TIME hook
+ * (BFAMO_KERNEL_RUN accumulating each kernel's time, GB/s and GFLOP/s into
+ * sc_statistics, src/bfam.h:1673-1708, src/bfam.c:8428-8475).  With
+ * profiling on (enable != 0; off by default) every stage launch of the
+ * domain is bracketed by a pair of CUDA events on its stream and steps run
+ * eagerly (no graph replay); bfam_gpu_domain_kernel_stats waits for the
+ * recorded launches and returns, per launch level (level 0: elements without
+ * coarse-side hanging faces), the launches, elements, device milliseconds,
+ * algorithmic bytes (FP64 q and dq streams: 32 bytes per DOF and stage, 24 in
+ * the first stage, 16 for a right-hand-side evaluation) and their GB/s.
+ * Enabling or disabling clears the totals.  Independently of this switch,
+ * each bfam_ts_lsrk_step and each LSRK stage is an NVTX range, for timeline
+ * tools. */
+typedef struct
+{
+  int level;
+  int64_t launches;
+  int64_t elements;
+  double ms;        /* device time summed over the launches */
+  double alg_bytes; /* algorithmic bytes summed over the launches */
+  double gbs;       /* alg_bytes / time */
+} bfam_gpu_kernel_stat_t;
+int bfam_gpu_domain_profile(bfam_gpu_domain_t *dom, int enable);
+int bfam_gpu_domain_kernel_stats(bfam_gpu_domain_t *dom,
+                                 bfam_gpu_kernel_stat_t *out, int max_levels,
+                                 int *nlevels);
+
 /* Domains and batches allocate from a stream-ordered memory pool that the
  * library creates per device and owns (other users of the device's default
  * pool are unaffected).  Freed blocks stay in that pool for the next domain;

@@ -176,6 +176,31 @@ def test_set_stream_orders_queued_steps():
     torch.cuda.synchronize()
 
 
+def test_per_launch_profile():
+    """Opt-in per-launch timing: per launch level, the launches, elements and
+    algorithmic bytes of the steps taken while it is on, and a positive
+    device time; the state is the same as without it."""
+    m, rho, lam, mu = _setup(3, 3, (4, 4, 4), 0.3, 0)
+    q0 = np.random.default_rng(5).standard_normal((m.nfields, m.K * m.Np))
+    dt = configs.stable_dt(m, rho, lam, mu, 0.4)
+    dom = bf.GpuDomain(m, rho, lam, mu)
+    dom.set_fields(q0)
+    ts = bf.LSRK(dom)
+    dom.profile(True)
+    ts.step(dt, 3, use_graph=True)   # eager while profiling
+    st = dom.kernel_stats()
+    dom.profile(False)
+    assert len(st) == dom.launch_levels() == 2
+    assert sum(s["elements"] for s in st) == 3 * 5 * m.K
+    assert all(s["launches"] == 15 and s["ms"] > 0 and s["gbs"] > 0 for s in st)
+    ndof = m.K * m.Np * m.nfields
+    assert abs(sum(s["alg_bytes"] for s in st) - 3 * (24 + 4 * 32) * ndof) < 1e-6 * ndof
+    ref = orc.Oracle.from_mesh(m, rho, lam, mu).lsrk(q0, dt, 3)
+    assert relerr(dom.get_fields(), ref).max() < TOL
+    ts.free()
+    dom.free()
+
+
 def test_library_pool_trim():
     m, rho, lam, mu = _setup(3, 3, (4, 4, 4), 0.3, 0)
     dom = bf.GpuDomain(m, rho, lam, mu)
