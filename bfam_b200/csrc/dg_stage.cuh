@@ -56,6 +56,28 @@ __device__ __forceinline__ int nth_bit(int m, int i)
   return __ffs(m) - 1;
 }
 
+// Node of thread t in the volume/update pass.  Nodes go in order (i
+// fastest), except in 3D when a k-plane holds between 32 and 64 nodes (N = 5,
+// 6): then warp w < Nq takes the first 32 nodes of plane w and the remaining
+// warps the rest of every plane, so that the lines along y a warp reads lie
+// in one plane (two planes per warp put lines of both at the same shared
+// memory banks).  Threads past the last node get Np.
+template <int DIM, int N, int NT>
+__device__ __forceinline__ int node_of_thread(int t)
+{
+  constexpr int Nq = N + 1, P = Nq * Nq, Np = DIM == 3 ? P * Nq : P;
+  if constexpr (DIM == 3 && P > 32 && P < 64 && NT >= Np)
+  {
+    if (t < 32 * Nq)
+      return (t >> 5) * P + (t & 31);
+    const int r = t - 32 * Nq;
+    constexpr int REST = P - 32;
+    return r < REST * Nq ? (r / REST) * P + 32 + r % REST : Np;
+  }
+  else
+    return t < Np ? t : Np;
+}
+
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
 // aligned).  NBUF element buffers (state, dq, face traces / lifted
 // contributions, face flux constants) let the loads of the next element fly
@@ -490,7 +512,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
 #pragma unroll 1
   for (int it = 0; it < NODE_ITERS; ++it)
   {
-    const int n = t + it * NT;
+    const int n = node_of_thread<DIM, N, NT>(t + it * NT);
     if (n >= Np)
       break;
     const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
