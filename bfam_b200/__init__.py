@@ -176,6 +176,7 @@ def _declare(L: C.CDLL) -> None:
         "bfam_gpu_batch_group_info": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int),
                                                 P(C.c_int), P(C.c_int64)]),
         "bfam_gpu_tile_count": (C.c_int, [C.c_int, C.c_int]),
+        "bfam_gpu_tile_elements": (C.c_int, [C.c_int, C.c_int, C.c_int]),
         "bfam_gpu_tile_shape": (C.c_int, [C.c_int, C.c_int, C.c_int, P(C.c_int),
                                           P(C.c_int)]),
         "bfam_gpu_batch_set_tile": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
@@ -608,13 +609,24 @@ class GpuDomain:
 
 
 def tile_shapes(dim: int, N: int) -> list[tuple[int, int]]:
-    """(threads per CTA, resident CTAs per SM) of each compiled tile."""
+    """(threads per element, resident CTAs per SM) of each compiled tile."""
     L = lib()
     out = []
     for t in range(L.bfam_gpu_tile_count(dim, N)):
         a, b = C.c_int(), C.c_int()
         _check(L.bfam_gpu_tile_shape(dim, N, t, C.byref(a), C.byref(b)))
         out.append((a.value, b.value))
+    return out
+
+
+def tile_elements(dim: int, N: int) -> list[int]:
+    """elements per CTA of each compiled tile"""
+    L = lib()
+    out = []
+    for t in range(L.bfam_gpu_tile_count(dim, N)):
+        e = L.bfam_gpu_tile_elements(dim, N, t)
+        _check(min(e, 0))
+        out.append(int(e))
     return out
 
 

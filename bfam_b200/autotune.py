@@ -1,9 +1,10 @@
 """Tile autotuner for batches.
 
-A batch runs one persistent launch per order group and LSRK stage.  The tile
-of a group is (threads per CTA, register budget for a number of resident
-CTAs per SM), chosen among the shapes compiled for that order
-(`tile_shapes`), plus the persistent grid's CTAs per SM.  The tuner times
+A batch runs one launch per order group, level and LSRK stage.  The tile of a
+group is (elements per CTA, threads per element, register budget for a
+number of resident CTAs per SM), chosen among the shapes compiled for that
+order (`tile_shapes`, `tile_elements`), plus the CTAs per SM of a persistent
+grid (two-buffer tiles) or of the L2 lookahead distance (one-buffer tiles).  The tuner times
 every candidate on a synthetic domain of the group's order, precision and
 roughly its element count (a 20 % refined brick, Gaussian pulse, random
 material, capped in size so tuning takes seconds), with CUDA events on the
@@ -19,7 +20,8 @@ from pathlib import Path
 
 import numpy as np
 
-from . import Batch, GpuDomain, Mesh, lgl_operators, material_random, tile_shapes
+from . import (Batch, BfamGpuError, GpuDomain, Mesh, lgl_operators, material_random,
+               tile_elements, tile_shapes)
 
 DEFAULT_CACHE = Path(__file__).resolve().parent / "tile_cache.json"
 MAX_TUNE_ELEMENTS = 24000
@@ -68,9 +70,13 @@ def tune_group(dim: int, N: int, precision: int, elements: int, steps: int = 4,
     b.set_stream(stream.cuda_stream)
     table = []
     shapes = tile_shapes(dim, N)
-    for tile, (threads, minb) in enumerate(shapes):
+    epcs = tile_elements(dim, N)
+    for tile, ((threads, minb), epc) in enumerate(zip(shapes, epcs)):
         for cps in sorted({0, max(1, minb - 1)} if minb > 1 else {0}):
-            b.set_tile(0, tile, cps)
+            try:
+                b.set_tile(0, tile, cps)
+            except BfamGpuError:
+                continue  # does not fit an SM on this device
             b.step([dt], 1)  # capture + warm-up
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -79,8 +85,8 @@ def tune_group(dim: int, N: int, precision: int, elements: int, steps: int = 4,
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / steps
-            table.append({"tile": tile, "threads": threads, "min_ctas": minb,
-                          "ctas_per_sm": cps, "ms_per_step": ms,
+            table.append({"tile": tile, "threads": threads, "elements_per_cta": epc,
+                          "min_ctas": minb, "ctas_per_sm": cps, "ms_per_step": ms,
                           "dof_updates_per_s": mesh.ndof * 5 / (ms / 1e3)})
     b.free()
     dom.free()
@@ -108,7 +114,7 @@ def autotune(batch: Batch, cache: dict | None = None, cache_path=None,
             dirty = True
         best = cache[key]["best"]
         batch.set_tile(g, best["tile"], best["ctas_per_sm"])
-        choices.append(dict(info, **best))
+        choices.append(dict(info, **best, table=cache[key].get("table", [])))
     if dirty and save and own_cache:
         save_cache(cache, cache_path)
     return choices

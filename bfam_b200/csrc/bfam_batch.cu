@@ -39,35 +39,37 @@ typedef int (*batch_occupancy_fn)();
 struct BatchTile
 {
   int NT = 0, MINB = 0, NBUF = 1;
+  int EPC = 1; // elements per CTA (NT threads each)
   batch_launch_fn launch = nullptr;
   batch_prepare_fn prepare = nullptr;
   batch_occupancy_fn occupancy = nullptr;
 };
 
-template <int DIM, int N, int NT, int MINB, typename CT> struct TileImpl
+template <int DIM, int N, int NT, int MINB, typename CT, int EPC = 1>
+struct TileImpl
 {
+  static constexpr int NB = EPC == 1 ? nbuf<DIM, N, CT>() : 1;
   static constexpr auto kernel =
-      dg_stage_batch_kernel<DIM, N, NT, MINB, MODE_STAGE, CT,
-                            nbuf<DIM, N, CT>()>;
+      dg_stage_batch_kernel<DIM, N, NT, MINB, MODE_STAGE, CT, NB, EPC>;
+  static constexpr size_t SMEM = stage_smem_bytes<DIM, N, CT, EPC>();
   static void launch(const DomainView *v, const int2 *w, int nwork,
                      const StageParams &sp, const double *hops, int grid,
                      cudaStream_t st)
   {
     const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
-    kernel<<<grid, NT, stage_smem_bytes<DIM, N, CT>(), st>>>(v, w, nwork, sp,
-                                                             dop);
+    kernel<<<grid, NT * EPC, SMEM, st>>>(v, w, nwork, sp, dop);
   }
   static cudaError_t prepare()
   {
     return cudaFuncSetAttribute((const void *)kernel,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)stage_smem_bytes<DIM, N, CT>());
+                                (int)SMEM);
   }
   static int occupancy()
   {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &n, kernel, NT, stage_smem_bytes<DIM, N, CT>()) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, NT * EPC,
+                                                      SMEM) != cudaSuccess)
     {
       cudaGetLastError();
       return 0;
@@ -79,7 +81,8 @@ template <int DIM, int N, int NT, int MINB, typename CT> struct TileImpl
     BatchTile t;
     t.NT = NT;
     t.MINB = MINB;
-    t.NBUF = nbuf<DIM, N, CT>();
+    t.EPC = EPC;
+    t.NBUF = NB;
     t.launch = launch;
     t.prepare = prepare;
     t.occupancy = occupancy;
@@ -95,16 +98,26 @@ template <typename CT> std::vector<BatchTile> tiles_for(int dim, int N)
 {
   std::vector<BatchTile> v;
 #define T(D, NN, NT, MB) v.push_back(TileImpl<D, NN, NT, MB, CT>::make())
+#define TE(D, NN, NT, MB, E) v.push_back(TileImpl<D, NN, NT, MB, CT, E>::make())
 #define T0(D, NN) T(D, NN, (Shape<D, NN>::NT), (stage_min_ctas<D, NN, CT>()))
   if (dim == 3)
   {
+    // beside one element per CTA: E elements per CTA of E x threads (each
+    // element its own tile and barrier), down to one warp per element at
+    // the low orders (register budget for the CTAs the shared memory admits)
     switch (N)
     {
-    case 1: T0(3, 1); break;
-    case 2: T0(3, 2); break;
-    case 3: T0(3, 3); T(3, 3, 96, 4); T(3, 3, 128, 4); break;
-    case 4: T0(3, 4); break;
-    case 5: T0(3, 5); T(3, 5, 224, 1); T(3, 5, 256, 2); break;
+    case 1: T0(3, 1); TE(3, 1, 32, 8, 4); TE(3, 1, 32, 4, 8); break;
+    case 2: T0(3, 2); TE(3, 2, 32, 8, 4); TE(3, 2, 64, 4, 2); break;
+    case 3:
+      T0(3, 3); T(3, 3, 96, 4); T(3, 3, 128, 4);
+      TE(3, 3, 96, 3, 2); TE(3, 3, 96, 2, 4); TE(3, 3, 32, 6, 4);
+      TE(3, 3, 64, 4, 4);
+      break;
+    case 4: T0(3, 4); TE(3, 4, 160, 2, 2); break;
+    case 5: T0(3, 5); T(3, 5, 224, 3); T(3, 5, 224, 1); T(3, 5, 256, 2);
+      TE(3, 5, 224, 2, 2);
+      break;
     case 6: T0(3, 6); break;
     case 7: T0(3, 7); T(3, 7, 384, 1); break;
     default: break;
@@ -126,6 +139,7 @@ template <typename CT> std::vector<BatchTile> tiles_for(int dim, int N)
     }
   }
 #undef T0
+#undef TE
 #undef T
   return v;
 }
@@ -366,10 +380,13 @@ int choose_grid(bfam_gpu_batch_t *b, bfam_gpu_batch_t::Group &g)
   // a persistent grid for two-buffer tiles; one CTA per work item for
   // one-buffer tiles
   const bool persistent = t.NBUF == 2;
-  g.ahead = persistent ? 0 : (int)std::min<int64_t>(full / 2, INT32_MAX);
+  // L2 lookahead in work items: half a wave of resident elements
+  g.ahead = persistent ? 0
+                       : (int)std::min<int64_t>(full * t.EPC / 2, INT32_MAX);
   g.grid.resize(g.nwork_l.size());
   for (size_t l = 0; l < g.nwork_l.size(); ++l)
-    g.grid[l] = (int)(persistent && g.nwork_l[l] > full ? full : g.nwork_l[l]);
+    g.grid[l] = (int)(persistent ? (g.nwork_l[l] > full ? full : g.nwork_l[l])
+                                 : (g.nwork_l[l] + t.EPC - 1) / t.EPC);
   return 0;
 }
 
@@ -715,6 +732,15 @@ int bfam_gpu_tile_shape(int dim, int N, int tile, int *threads, int *min_ctas)
   *threads = t[tile].NT;
   *min_ctas = t[tile].MINB;
   return 0;
+}
+
+int bfam_gpu_tile_elements(int dim, int N, int tile)
+{
+  const auto t = tiles(dim, N, BFAM_GPU_PRECISION_FP64);
+  if (tile < 0 || tile >= (int)t.size())
+    return fail(BFAM_GPU_EINVAL, "no tile %d for dim %d order %d", tile, dim,
+                N);
+  return t[tile].EPC;
 }
 
 // ---------------------------------------------------------------- batch

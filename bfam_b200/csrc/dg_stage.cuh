@@ -137,8 +137,46 @@ template <int DIM, int N, typename CT> __host__ __device__ constexpr int nbuf()
              : 1;
 }
 
+// Elements per CTA: a CTA of EPC * NT threads holds EPC sub-elements of NT
+// threads, each with its own shared-memory tile (Tile::TOTAL doubles, one
+// after the other) and its own barrier -- the CTA's barrier when EPC = 1, the
+// warp's when NT = 32, else named barrier 1 + sub -- so that sub-elements
+// whose branches differ (fine or coarse faces) never wait for each other.
+template <int NT, int EPC> struct Sub
+{
+  static_assert(EPC >= 1 && (EPC == 1 || NT == 32 || EPC <= 15),
+                "named barriers 1..15");
+  static_assert(NT % 32 == 0, "whole warps per sub-element");
+  __device__ __forceinline__ static int t()
+  {
+    return EPC == 1 ? (int)threadIdx.x : (int)threadIdx.x % NT;
+  }
+  __device__ __forceinline__ static int id()
+  {
+    return EPC == 1 ? 0 : (int)threadIdx.x / NT;
+  }
+  __device__ __forceinline__ static void sync()
+  {
+    if constexpr (EPC == 1)
+      __syncthreads();
+    else if constexpr (NT == 32)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + id()), "n"(NT) : "memory");
+  }
+};
+
+// shared-memory tile of this thread's sub-element
+template <typename T, int NT, int EPC>
+__device__ __forceinline__ double *sub_smem()
+{
+  extern __shared__ __align__(16) double smem[];
+  return EPC == 1 ? smem : smem + Sub<NT, EPC>::id() * T::TOTAL;
+}
+
 // Element buffer b of the tile.
-template <int DIM, int N, typename CT, int NBUF> struct TileBuf
+template <int DIM, int N, typename CT, int NBUF, int NT = 32, int EPC = 1>
+struct TileBuf
 {
   double *qs, *R, *pt, *fcf;
   uint64_t *bq, *bdq;
@@ -147,7 +185,7 @@ template <int DIM, int N, typename CT, int NBUF> struct TileBuf
     using S = Shape<DIM, N>;
     constexpr bool DQS = stage_dqs<DIM, N, CT>();
     using T = Tile<DIM, N, CT, NBUF, DQS>;
-    extern __shared__ __align__(16) double smem[];
+    double *smem = sub_smem<T, NT, EPC>();
     qs = smem + b * T::BUF;
     R = qs + S::SM_QS;
     pt = R + (DQS ? S::SM_DQ : 0);
@@ -161,7 +199,8 @@ template <int DIM, int N, typename CT, int NBUF> struct TileBuf
 // stage) dq by TMA bulk copies completing on the buffer's mbarriers, the
 // neighbours' face traces and the face flux constants by cp.async, as one
 // commit group.
-template <int DIM, int N, int NT, int MODE, typename CT, int NBUF>
+template <int DIM, int N, int NT, int MODE, typename CT, int NBUF,
+          int EPC = 1>
 __device__ __forceinline__ void issue_element(const DomainView &d,
                                               const StageParams &sp, int e,
                                               int b)
@@ -169,10 +208,10 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
   using S = Shape<DIM, N>;
   constexpr int Np = S::Np, Nfp = S::Nfp, NF = S::NF, NFLD = S::NFLD,
                 NTF = S::NTF;
-  const TileBuf<DIM, N, CT, NBUF> tb(b);
+  const TileBuf<DIM, N, CT, NBUF, NT, EPC> tb(b);
   double *qs = tb.qs, *R = tb.R, *pt = tb.pt, *fcf = tb.fcf;
   uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
-  const int t = threadIdx.x;
+  const int t = Sub<NT, EPC>::t();
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
   const bool rd = MODE != MODE_RHS && !sp.first_stage;
@@ -290,7 +329,8 @@ __device__ __forceinline__ void prefetch_element(const DomainView &d,
 
 // Compute element e from buffer b (its loads issued by issue_element; `par`
 // is the buffer's mbarrier phase parity).
-template <int DIM, int N, int NT, int MODE, typename CT, int NBUF>
+template <int DIM, int N, int NT, int MODE, typename CT, int NBUF,
+          int EPC = 1>
 __device__ __forceinline__ void compute_element(const DomainView &d,
                                                 const StageParams &sp,
                                                 const DiffOp<N, CT> &dop,
@@ -301,11 +341,11 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   constexpr int Nq = S::Nq, Np = S::Np, Nfp = S::Nfp, NF = S::NF,
                 NFLD = S::NFLD, NJ = S::NJ, NPC = S::NPC, ROWS = S::ROWS,
                 NTF = S::NTF;
-  static_assert(NT >= NF * Nfp, "one face-node work item per thread");
-  // the dynamic shared array itself (not a pointer parameter), so that all
-  // accesses stay in the shared window with 32-bit addressing
-  extern __shared__ __align__(16) double smem[];
-  const TileBuf<DIM, N, CT, NBUF> tb(b);
+  // this sub-element's tile, derived from the dynamic shared array itself
+  // (not a pointer parameter), so that all accesses stay in the shared
+  // window with 32-bit addressing
+  double *smem = sub_smem<T, NT, EPC>();
+  const TileBuf<DIM, N, CT, NBUF, NT, EPC> tb(b);
   double *qs = tb.qs, *R = tb.R, *pt = tb.pt, *fcf = tb.fcf;
   uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
   double *mj = smem + T::OFF_MJ; // [DIM][NJ][Nfp] coarse-side jumps, by fine rank
@@ -322,7 +362,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   else
     qv = qs;
 
-  const int t = threadIdx.x;
+  const int t = Sub<NT, EPC>::t();
   const size_t fs = d.fs;
   const size_t eoff = (size_t)e * Np;
   // the update is dq = a dq + s rhs; the right-hand-side mode uses a = 0, s = 1
@@ -350,13 +390,13 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   }
   cp_async_wait<NBUF - 1>(); // this element's group (the next one may fly)
   if constexpr (NARROW && !S::TMA)
-    __syncthreads(); // other threads' cp.async writes of q
+    Sub<NT, EPC>::sync(); // other threads' cp.async writes of q
   if constexpr (NARROW)
   {
     for (int w = t; w < NFLD * Np; w += NT)
       qv[w] = CT(qs[w] - qs[(w / Np) * Np]);
   }
-  __syncthreads();
+  Sub<NT, EPC>::sync();
   // lift factor of face axis ax: s (2/h_ax) / w_0
   auto lfac = [&](int ax) {
     return CT(s * (ax == 0 ? me.rx : (ax == 1 ? me.ry : me.rz)) * dop.iwend);
@@ -380,7 +420,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         else
           line_apply<N, false, CT, CT>(dop, half, x + line, Nq);
       }
-      __syncthreads();
+      Sub<NT, EPC>::sync();
     }
   }
 
@@ -392,11 +432,11 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   //   coarse (T* - T-) = -(fine J_T) + [T],  coarse (v* - v-) = fine J_v - [v]
   // with [.] = coarse - fine as seen from the fine side; they go to mj in the
   // coarse piece's node order.
+  for (int w = t; w < NF * Nfp; w += NT)
   {
     CT lc[NFLD];
-    if (t < NF * Nfp)
     {
-      const int f = t / Nfp, pn = t % Nfp;
+      const int f = w / Nfp, pn = w % Nfp;
       const int y = desc[f].y;
       const int k = y & 3;
       if (k != 2)
@@ -466,7 +506,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   // (FP64), then out to the mortar buffer for the coarse element
   if (nfine)
   {
-    __syncthreads();
+    Sub<NT, EPC>::sync();
     for (int w = t; w < nfine * NJ * ROWS; w += NT)
     {
       const int fr = w / (NJ * ROWS), r = w % (NJ * ROWS);
@@ -475,7 +515,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       line_apply_s<N, false, double, double>(
           sPb, (hp - 1) & 1, mj + (fr * NJ + c) * Nfp + Nq * line, 1);
     }
-    __syncthreads();
+    Sub<NT, EPC>::sync();
     if (DIM == 3)
     {
       for (int w = t; w < nfine * NJ * Nq; w += NT)
@@ -486,7 +526,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         line_apply_s<N, false, double, double>(
             sPb, (hp - 1) >> 1, mj + (fr * NJ + c) * Nfp + col, Nq);
       }
-      __syncthreads();
+      Sub<NT, EPC>::sync();
     }
     for (int w = t; w < nfine * NJ * Nfp; w += NT)
     {
@@ -496,7 +536,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
           mj[fr * NJ * Nfp + r];
     }
   }
-  __syncthreads();
+  Sub<NT, EPC>::sync();
 
   // ------------------------ phase 2: volume, face contributions and update
   constexpr bool DQS = stage_dqs<DIM, N, CT>();
@@ -588,15 +628,18 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
 // blockIdx.x, blockIdx.x + gridDim.x, ...) and the loads of the next item
 // are issued before the current one is computed.
 template <int DIM, int N, int NT, int MODE, typename CT, int NBUF,
-          typename Item>
+          typename Item, int EPC = 1>
 __device__ __forceinline__ void stage_loop(const Item &item, int n,
                                            const StageParams &sp,
                                            const DiffOp<N, CT> &dop)
 {
   using T = Tile<DIM, N, CT, NBUF, stage_dqs<DIM, N, CT>()>;
+  using SB = Sub<NT, EPC>;
+  static_assert(EPC == 1 || NBUF == 1, "sub-elements use one buffer each");
   constexpr int Nq = N + 1;
-  extern __shared__ __align__(16) double smem[];
-  if (threadIdx.x == 0)
+  double *smem = sub_smem<T, NT, EPC>();
+  const int lt = SB::t();
+  if (lt == 0)
   {
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem + T::OFF_BAR);
     for (int i = 0; i < 2 * NBUF; ++i)
@@ -607,29 +650,29 @@ __device__ __forceinline__ void stage_loop(const Item &item, int n,
     CT *sD = reinterpret_cast<CT *>(smem + T::OFF_OPS);
     CT *sIb = reinterpret_cast<CT *>(smem + T::OFF_OPS + Nq * Nq);
     double *sPb = smem + T::OFF_OPS + 2 * Nq * Nq;
-    for (int w = threadIdx.x; w < Nq * Nq; w += NT)
+    for (int w = lt; w < Nq * Nq; w += NT)
     {
       sD[w] = dop.D[w];
       sIb[w] = dop.Ib[w];
       sPb[w] = dop.Pb[w];
     }
   }
-  __syncthreads();
-  int idx = blockIdx.x;
+  SB::sync();
+  int idx = (int)blockIdx.x * EPC + SB::id();
   if (idx >= n)
     return;
   if constexpr (NBUF == 1)
   {
-    // one element per CTA (the grid covers every item)
-    issue_element<DIM, N, NT, MODE, CT, 1>(item.view(idx), sp, item.elem(idx),
-                                           0);
+    // one element per sub-element (the grid covers every item)
+    issue_element<DIM, N, NT, MODE, CT, 1, EPC>(item.view(idx), sp,
+                                                item.elem(idx), 0);
     // a thread of another warp than the TMA issuer prefetches a later
     // item's element while this one's loads fly
     const int ia = idx + sp.ahead;
-    if (sp.ahead > 0 && ia < n && threadIdx.x == (NT > 32 ? 32 : 0))
+    if (sp.ahead > 0 && ia < n && lt == (NT > 32 ? 32 : 0))
       prefetch_element<DIM, N, MODE>(item.view(ia), sp, item.elem(ia));
-    compute_element<DIM, N, NT, MODE, CT, 1>(item.view(idx), sp, dop,
-                                             item.elem(idx), 0, 0);
+    compute_element<DIM, N, NT, MODE, CT, 1, EPC>(item.view(idx), sp, dop,
+                                                  item.elem(idx), 0, 0);
     return;
   }
   issue_element<DIM, N, NT, MODE, CT, NBUF>(item.view(idx), sp,
@@ -686,23 +729,28 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 // Many domains of the same order: item idx is work[idx] = (domain, element),
-// each domain with its own arrays and time step.
-template <int DIM, int N, int NT, int MINB, int MODE, typename CT, int NBUF>
-__global__ void __launch_bounds__(NT, MINB)
+// each domain with its own arrays and time step.  EPC elements per CTA of
+// EPC * NT threads (one buffer each).
+template <int DIM, int N, int NT, int MINB, int MODE, typename CT, int NBUF,
+          int EPC = 1>
+__global__ void __launch_bounds__(NT *EPC, MINB)
     dg_stage_batch_kernel(const DomainView *__restrict__ views,
                           const int2 *__restrict__ work, int nwork,
                           StageParams sp,
                           const __grid_constant__ DiffOp<N, CT> dop)
 {
-  stage_loop<DIM, N, NT, MODE, CT, NBUF>(BatchItems{views, work}, nwork, sp,
-                                         dop);
+  stage_loop<DIM, N, NT, MODE, CT, NBUF, BatchItems, EPC>(
+      BatchItems{views, work}, nwork, sp, dop);
 }
 
-// dynamic shared memory of one CTA of the stage kernels
-template <int DIM, int N, typename CT>
+// dynamic shared memory of one CTA of the stage kernels (EPC sub-elements of
+// one buffer each when EPC > 1)
+template <int DIM, int N, typename CT, int EPC = 1>
 __host__ __device__ constexpr size_t stage_smem_bytes()
 {
-  return Tile<DIM, N, CT, nbuf<DIM, N, CT>(), stage_dqs<DIM, N, CT>()>::BYTES;
+  return EPC == 1
+             ? Tile<DIM, N, CT, nbuf<DIM, N, CT>(), stage_dqs<DIM, N, CT>()>::BYTES
+             : EPC * Tile<DIM, N, CT, 1, stage_dqs<DIM, N, CT>()>::BYTES;
 }
 
 // resident CTAs per SM the register budget is sized for: the shape's choice,

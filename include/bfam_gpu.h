@@ -235,6 +235,9 @@ int bfam_gpu_domain_energy(bfam_gpu_domain_t *dom, double *energy);
  * whose work overlaps on the GPU (different streams or devices sharing a
  * context) race and may return wrong values -- serialise them.  Every element
  * slot is rewritten by each call, so no clearing is needed between calls. */
+/* The address is looked up once per device ordinal and kept for the process:
+ * this assumes the device's primary context and no cudaDeviceReset in
+ * between. */
 #define BFAM_GPU_NOALLOC_MAX_ELEMENTS 262144
 int bfam_gpu_domain_energy_noalloc(bfam_gpu_domain_t *dom, double *energy);
 
@@ -420,13 +423,17 @@ int bfam_gpu_pglue_free(bfam_gpu_pglue_t *g);
  * added glue when the batch steps. */
 int bfam_gpu_batch_add_pglue(bfam_gpu_batch_t *b, bfam_gpu_pglue_t *g);
 
-/* Tile shapes compiled for an order: tile t has `threads` threads per CTA
- * (one element per CTA, one thread per node and per face node; a tile with
- * fewer threads than nodes loops over the nodes) and a register budget for
- * `min_ctas` resident CTAs per SM.  Tile 0 is the single-domain kernel's. */
+/* Tile shapes compiled for an order: tile t runs bfam_gpu_tile_elements
+ * elements per CTA with `threads` threads each (a tile with fewer threads
+ * than nodes or face nodes loops over them; each element of a CTA has its
+ * own shared-memory tile and barrier, down to one warp per element) and a
+ * register budget for `min_ctas` resident CTAs per SM.  Tile 0 is the
+ * single-domain kernel's (one element per CTA). */
 int bfam_gpu_tile_count(int dim, int N);
 int bfam_gpu_tile_shape(int dim, int N, int tile, int *threads,
                         int *min_ctas);
+/* elements per CTA of tile t (>= 1), or a negative BFAM_GPU_E* code */
+int bfam_gpu_tile_elements(int dim, int N, int tile);
 /* Choose group g's tile and persistent grid (ctas_per_sm CTAs per SM; 0:
  * as many as fit). */
 int bfam_gpu_batch_set_tile(bfam_gpu_batch_t *b, int g, int tile,

@@ -213,16 +213,22 @@ def test_batch_and_extras_reject_bad_arguments_without_a_device():
 
 
 def test_tile_table():
-    # tile 0 is the single-domain kernel's shape; every tile has one thread
-    # per face node at least
+    # tile 0 is the single-domain kernel's shape (one element per CTA, one
+    # thread per face node at least); the others may put several elements
+    # in a CTA, down to one warp per element
     for dim, orders in ((2, range(1, 9)), (3, range(1, 8))):
         for N in orders:
             shapes = bf.tile_shapes(dim, N)
-            assert shapes, (dim, N)
+            epc = bf.tile_elements(dim, N)
+            assert shapes and len(epc) == len(shapes), (dim, N)
             nfp = (N + 1) ** (dim - 1)
-            for threads, minb in shapes:
-                assert threads % 32 == 0 and threads >= 2 * dim * nfp and minb >= 1
-    assert len(bf.tile_shapes(3, 5)) == 3 and len(bf.tile_shapes(3, 7)) == 2
+            assert shapes[0][0] >= 2 * dim * nfp and epc[0] == 1
+            for (threads, minb), e in zip(shapes, epc):
+                assert threads % 32 == 0 and minb >= 1 and e >= 1
+                assert threads * e <= 1024
+    assert bf.tile_elements(3, 3).count(1) == 3 and max(bf.tile_elements(3, 3)) == 4
+    assert len(bf.tile_shapes(3, 5)) == 5 and len(bf.tile_shapes(3, 7)) == 2
     assert bf.lib().bfam_gpu_tile_count(3, 9) == 0
     a, b = C.c_int(), C.c_int()
     assert bf.lib().bfam_gpu_tile_shape(3, 5, 7, C.byref(a), C.byref(b)) == bf.BFAM_GPU_EINVAL
+    assert bf.lib().bfam_gpu_tile_elements(3, 5, 7) == bf.BFAM_GPU_EINVAL

@@ -104,8 +104,12 @@ def test_batch_graph_equals_eager_and_steps_continue():
 
 
 def test_every_tile_gives_the_same_result():
+    """every compiled tile -- one element per CTA with any register budget,
+    several elements per CTA, one warp per element -- steps bitwise alike"""
     cases = [(3, 3, (4, 4, 4), 0.3, 1, 0), (3, 5, (3, 3, 3), 0.3, 2, 0),
-             (3, 7, (2, 2, 2), 0.5, 3, 0), (3, 5, (3, 3, 3), 0.3, 2, 1)]
+             (3, 7, (2, 2, 2), 0.5, 3, 0), (3, 5, (3, 3, 3), 0.3, 2, 1),
+             (3, 1, (3, 3, 3), 0.4, 4, 0), (3, 2, (3, 2, 3), 0.4, 5, 0),
+             (3, 3, (3, 3, 3), 0.5, 6, 1), (3, 4, (2, 3, 2), 0.5, 7, 0)]
     for c in cases:
         m, rho, lam, mu, q0, dt = _problem(*c)
         out = []
@@ -200,3 +204,33 @@ def test_source_outside_the_mesh_is_rejected():
     assert ei.value.code == bf.BFAM_GPU_EINVAL
     with pytest.raises(bf.BfamGpuError):
         d.set_receivers(np.array([[0.5, -0.1, 0.5]]), 4)
+
+
+def test_elements_per_cta_tiles_across_domains():
+    """a CTA's elements may belong to different domains (uneven counts, so
+    that CTAs straddle domain boundaries and the last CTA is partly empty):
+    each domain equals itself stepped alone and the oracle"""
+    meshes = [bf.Mesh(3, 3, n, refine_prob=0.4, seed=s)
+              for n, s in (((3, 3, 3), 11), ((2, 3, 2), 12), ((1, 1, 3), 13))]
+    probs = []
+    for k, m in enumerate(meshes):
+        rho, lam, mu = bf.material_random(m.K, 20 + k)
+        q0 = np.random.default_rng(k).standard_normal((m.nfields, m.K * m.Np))
+        probs.append((m, rho, lam, mu, q0))
+    dt = min(configs.stable_dt(m, r, l, u, 0.4) for m, r, l, u, _ in probs)
+    epc = bf.tile_elements(3, 3)
+    for tile in [t for t, e in enumerate(epc) if e > 1]:
+        doms = []
+        for m, rho, lam, mu, q0 in probs:
+            d = bf.GpuDomain(m, rho, lam, mu)
+            d.set_fields(q0)
+            doms.append(d)
+        b = bf.Batch(doms)
+        b.set_tile(0, tile, 0)
+        b.step([dt] * len(doms), 3)
+        for d, (m, rho, lam, mu, q0) in zip(doms, probs):
+            ref = orc.Oracle.from_mesh(m, rho, lam, mu).lsrk(q0, dt, 3)
+            assert relerr(d.get_fields(), ref).max() < 1e-12, (tile, m.K)
+        b.free()
+        for d in doms:
+            d.free()
