@@ -134,17 +134,26 @@ template <int DIM, int N> struct Shape
   // and row a of the stress (traction = sg * row a)
   static constexpr int NTF = 2 * DIM;
   static constexpr int ROWS = DIM == 3 ? Nq : 1; // rows of a face
-  static constexpr int NL = Np / Nq;              // lines per direction
-  static constexpr int NDF = DIM == 3 ? 6 : 4; // fields differentiated per axis
+  // Node-group volume pass (3D, even Nq): a thread owns GQJ x GQK nodes
+  // mirrored in j and k (see group_normal); GROUP_NT threads cover them,
+  // whole warps, 0 where the pass is not used.  3D N=5: node pairs (k,
+  // N-k), 108 threads in four warps.
+  static constexpr int GQJ = 1, GQK = 2;
+  static constexpr int GROUP_NT =
+      0;
   // one thread per node, or per face node where those are fewer (3D N=7:
-  // 384 face nodes, 512 nodes in two passes, so that two CTAs fit an SM)
+  // 384 face nodes, 512 nodes in two passes, so that two CTAs fit an SM),
+  // or the node-group pass's threads
   static constexpr int work =
-      (DIM == 3 && N == 7) ? NF * Nfp : (Np > NF * Nfp ? Np : NF * Nfp);
+      GROUP_NT ? GROUP_NT
+               : ((DIM == 3 && N == 7) ? NF * Nfp
+                                       : (Np > NF * Nfp ? Np : NF * Nfp));
   static constexpr int NT = ((work + 31) / 32) * 32 > 1024
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
   // CTAs per SM the register allocation is sized for (about 96 registers;
-  // 3D N=5: four CTAs of 224 threads at 72 registers, with dq read from L2)
+  // 3D N=5: seven CTAs of 128 threads at 72 registers, as many as the
+  // shared memory admits, with dq read from L2)
   static constexpr int MINB_RAW = 65536 / (NT * 96);
   static constexpr int MINB = (DIM == 3 && N == 7)
                                   ? 2
@@ -158,18 +167,16 @@ template <int DIM, int N> struct Shape
   // shared memory regions in doubles (all even, so 16-byte aligned)
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q
   static constexpr int SM_DQ = SM_QS; // dq, then A dq + dt rhs in place
-  static constexpr int SM_PT = NF * NFLD * Nfp + (NF * NFLD * Nfp) % 2;
+  // per face: the neighbour's NTF trace fields, then in place the NJ flux
+  // jumps of each face node (NJ == NTF)
+  static constexpr int SM_PT = NF * NTF * Nfp + (NF * NTF * Nfp) % 2;
   // coarse-side jumps of the fine faces, projected in place; an element has
   // at most DIM faces on the fine side of a hanging face (those on its
   // parent's boundary)
   static constexpr int SM_MJ = DIM * NJ * Nfp + (DIM * NJ * Nfp) % 2;
-  // face flux constants, then the element record (ElemData)
-  static constexpr int SM_FC = 4 * NF + 8;
   // differentiation matrix, bottom-half mortar interpolation and projection
   // (Nq*Nq entries each, one double slot per entry)
   static constexpr int SM_IP = 3 * Nq * Nq + (Nq % 2);
-  static constexpr int SM_TOTAL =
-      SM_QS + SM_DQ + SM_PT + SM_MJ + SM_FC + SM_IP + 4;
   // precision form only: FP32 copy of q minus the element's first node,
   // after the mbarriers
   static constexpr int SM_QF = (NFLD * Np + 3) / 4 * 2;

@@ -78,6 +78,55 @@ __device__ __forceinline__ int node_of_thread(int t)
     return t < Np ? t : Np;
 }
 
+// The node-group volume pass runs where the shape provides it and the CTA
+// (or sub-element) has its thread count.
+template <int DIM, int N, int NT> __host__ __device__ constexpr bool group_pass()
+{
+  return Shape<DIM, N>::GROUP_NT != 0 && NT == Shape<DIM, N>::GROUP_NT;
+}
+
+// Nodes of thread t in the node-group pass: (i, j, k) with j < Nq/2 if
+// paired in j, k < Nq/2 if paired in k.  As in node_of_thread, when a plane
+// of the (i, j) range holds between 32 and 64 of them, warp w takes the
+// first 32 of plane w and the last warp the rest of every plane.  False for
+// threads without nodes.
+template <int DIM, int N, int NT>
+__device__ __forceinline__ bool group_of_thread(int t, int &i, int &j, int &k)
+{
+  using S = Shape<DIM, N>;
+  constexpr int Nq = S::Nq;
+  constexpr int P = (S::GQJ == 2 ? Nq / 2 : Nq) * Nq;
+  constexpr int KP = S::GQK == 2 ? Nq / 2 : Nq;
+  int p, plane;
+  if constexpr (P > 32 && P < 64)
+  {
+    if (t < 32 * KP)
+    {
+      plane = t >> 5;
+      p = t & 31;
+    }
+    else
+    {
+      const int r = t - 32 * KP;
+      if (r >= (P - 32) * KP)
+        return false;
+      plane = r / (P - 32);
+      p = 32 + r % (P - 32);
+    }
+  }
+  else
+  {
+    if (t >= P * KP)
+      return false;
+    plane = t / P;
+    p = t % P;
+  }
+  i = p % Nq;
+  j = p / Nq;
+  k = plane;
+  return true;
+}
+
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
 // aligned).  NBUF element buffers (state, dq, face traces / lifted
 // contributions, face flux constants) let the loads of the next element fly
@@ -270,7 +319,7 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
       // trees: the host refuses any other pairing or orientation)
       const int src_n = gmask<DIM, N>((ds.y >> 2) & 7, pn);
       const double *src = d.qin + (size_t)ds.x * Np + src_n;
-      double *dst = pt + f * NFLD * Nfp + pn;
+      double *dst = pt + f * NTF * Nfp + pn;
 #pragma unroll
       for (int c = 0; c < NTF; ++c)
         cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
@@ -398,9 +447,11 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   }
   Sub<NT, EPC>::sync();
   // lift factor of face axis ax: s (2/h_ax) / w_0
-  auto lfac = [&](int ax) {
-    return CT(s * (ax == 0 ? me.rx : (ax == 1 ? me.ry : me.rz)) * dop.iwend);
-  };
+  CT lfac[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax)
+    lfac[ax] =
+        CT(s * (ax == 0 ? me.rx : (ax == 1 ? me.ry : me.rz)) * dop.iwend);
 
   // fine side: coarse partner trace -> my piece, in place (rows, then columns)
   if (nfine)
@@ -414,7 +465,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int hp = (desc[f].y >> 8) & 7;
         const int c = r / ROWS, line = r % ROWS;
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
-        double *x = pt + (f * NFLD + c) * Nfp;
+        double *x = pt + (f * NTF + c) * Nfp;
         if (pass == 0)
           line_apply<N, false, CT, CT>(dop, half, x + Nq * line, 1);
         else
@@ -424,17 +475,16 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
     }
   }
 
-  // flux on conforming and fine-side faces, lifted to the face node's field
-  // contributions, written in place over the node's own trace slots (a
-  // thread reads only its own node's slots: partners' face nodes are in the
-  // same order on aligned trees).  On a fine face the coarse side's jumps follow from the same Riemann
+  // flux on conforming and fine-side faces: the face node's jumps (T* - T-,
+  // v* - v-), written in place over the node's own trace slots (a thread
+  // reads only its own node's slots: partners' face nodes are in the same
+  // order on aligned trees) and lifted by the node pass.  On a fine face the coarse side's jumps follow from the same Riemann
   // solution (star state v*, S* n shared by both sides, coarse normal -n):
   //   coarse (T* - T-) = -(fine J_T) + [T],  coarse (v* - v-) = fine J_v - [v]
   // with [.] = coarse - fine as seen from the fine side; they go to mj in the
   // coarse piece's node order.
   for (int w = t; w < NF * Nfp; w += NT)
   {
-    CT lc[NFLD];
     {
       const int f = w / Nfp, pn = w % Nfp;
       const int y = desc[f].y;
@@ -444,7 +494,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int vm = gmask<DIM, N>(f, pn);
         const int pp = pn;
         CT dq[NTF], J[6];
-        const double *x = pt + f * NFLD * Nfp;
+        double *x = pt + f * NTF * Nfp;
         // boundary faces: ghost state v+ = v-, S+ = -S- (free surface) or
         // q+ = 0 (absorbing)
         const bool free_surface = k == 3 && ((y >> 2) & 3) == 0;
@@ -472,20 +522,19 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
             m[c * Nfp] = double(v);
           }
         }
-        lift_face<DIM, CT>(J, f >> 1, sg, lfac(f >> 1), me, lc);
 #pragma unroll
-        for (int c = 0; c < NFLD; ++c)
-          pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
+        for (int c = 0; c < NJ; ++c)
+          x[c * Nfp + pp] = double(J[jslot<DIM>(c)]);
       }
     }
   }
 
-  // coarse side: the pieces' projected jumps, summed in glue order, lifted
+  // coarse side: the pieces' projected jumps, summed in glue order (stored
+  // at the precision of the right-hand side, like the flux jumps)
   for (int w = t; MODE != MODE_STAGE_NC && w < ncoarse * Nfp; w += NT)
   {
     const int f = nth_bit(coarse_mask, w / Nfp), pn = w % Nfp;
     const double *mb = d.mbuf + (size_t)desc[f].x * NJ * Nfp + pn;
-    CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
     for (int c = 0; c < NJ; ++c)
     {
@@ -493,13 +542,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
 #pragma unroll
       for (int p = 0; p < NPC; ++p)
         sum += mb[(p * NJ + c) * Nfp];
-      J[jslot<DIM>(c)] = CT(sum);
+      pt[(f * NTF + c) * Nfp + pn] = double(CT(sum));
     }
-    lift_face<DIM, CT>(J, f >> 1, (f & 1) ? CT(1) : CT(-1), lfac(f >> 1), me,
-                       lc);
-#pragma unroll
-    for (int c = 0; c < NFLD; ++c)
-      pt[(f * NFLD + c) * Nfp + pn] = double(lc[c]);
   }
 
   // fine side: L2 projection of the coarse-side jumps to the coarse face
@@ -548,53 +592,44 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         atomicExch(d.err, 2);
     }
   }
-  constexpr int NODE_ITERS = (Np + NT - 1) / NT;
-#pragma unroll 1
-  for (int it = 0; it < NODE_ITERS; ++it)
-  {
-    const int n = node_of_thread<DIM, N, NT>(t + it * NT);
-    if (n >= Np)
-      break;
-    const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
-    double acc[NFLD];
-    if constexpr (!NARROW)
-    {
-      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
-    }
-    else
-    {
-      CT rv[NFLD];
-      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
+  // Finish node n = (i, j, k) for fields [C0, C1), acc[c - C0] holding s
+  // times its volume right-hand side: the lifted jumps of the faces it lies
+  // on (at most one per axis, in face order), the point source, then the
+  // stage update (or the right-hand side out).  Every node pass goes
+  // through here.
+  auto finish = [&](auto c0, auto c1, int n, int i, int j, int k,
+                    double *acc) {
+    constexpr int C0 = decltype(c0)::value, C1 = decltype(c1)::value;
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        acc[c] = double(rv[c]);
-    }
-
-    // lifted face contributions of the faces this node lies on
-#pragma unroll
-    for (int f = 0; f < NF; ++f)
+    for (int ax = 0; ax < DIM; ++ax)
     {
-      const int ax = f >> 1, side = f & 1;
       const int idx = ax == 0 ? i : (ax == 1 ? j : k);
-      if (idx != (side ? N : 0))
+      if (idx != 0 && idx != N)
         continue;
+      const int side = idx == N;
+      const int f = 2 * ax + side;
       const int pn = DIM == 3 ? (ax == 0 ? j + Nq * k
                                          : (ax == 1 ? i + Nq * k : i + Nq * j))
                               : (ax == 0 ? j : i);
-      const double *lc = pt + f * NFLD * Nfp + pn;
+      const double *jp = pt + f * NTF * Nfp + pn;
+      CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        acc[c] += lc[c * Nfp];
+      for (int c = 0; c < NJ; ++c)
+        J[jslot<DIM>(c)] = CT(jp[c * Nfp]);
+      lift_face<DIM, CT>(J, ax, side ? CT(1) : CT(-1), lfac[ax], me, lc);
+#pragma unroll
+      for (int c = C0; c < C1; ++c)
+        acc[c - C0] += double(lc[c]);
     }
 
     // point source on the velocity: s f(t_stage) F phi_n(x_s) / (rho w_n J)
-    if (e == d.src.elem)
+    if (C0 < DIM && e == d.src.elem)
     {
       const double ts = d.clock->time + sp.C * d.dt;
       const double g = s * ricker(ts, d.src.f0, d.src.t0) * d.src.w[n] * me.irho;
 #pragma unroll
-      for (int c = 0; c < DIM; ++c)
-        acc[c] += g * d.src.force[c];
+      for (int c = C0; c < (C1 < DIM ? C1 : DIM); ++c)
+        acc[c - C0] += g * d.src.force[c];
     }
 
     if constexpr (MODE != MODE_RHS)
@@ -602,21 +637,92 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       if (rd)
       {
 #pragma unroll
-        for (int c = 0; c < NFLD; ++c)
-          acc[c] += a * (DQS ? R[c * Np + n] : d.dq[c * fs + eoff + n]);
+        for (int c = C0; c < C1; ++c)
+          acc[c - C0] +=
+              a * (DQS ? R[c * Np + n] : d.dq[c * fs + eoff + n]);
       }
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
+      for (int c = C0; c < C1; ++c)
       {
-        d.dq[c * fs + eoff + n] = acc[c];
-        d.qout[c * fs + eoff + n] = qs[c * Np + n] + sp.B * acc[c];
+        d.dq[c * fs + eoff + n] = acc[c - C0];
+        d.qout[c * fs + eoff + n] = qs[c * Np + n] + sp.B * acc[c - C0];
       }
     }
     else
     {
 #pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        d.rhs[c * fs + eoff + n] = acc[c];
+      for (int c = C0; c < C1; ++c)
+        d.rhs[c * fs + eoff + n] = acc[c - C0];
+    }
+  };
+  using I0 = std::integral_constant<int, 0>;
+
+  if constexpr (group_pass<DIM, N, NT>())
+  {
+    // node groups (see group_normal): normal stress, shear stress, velocity
+    constexpr int QJ = S::GQJ, QK = S::GQK, G = QJ * QK;
+    int i, j, k;
+    if (group_of_thread<DIM, N, NT>(t, i, j, k))
+    {
+      auto group = [&](auto c0, const CT (*rg)[3]) {
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+        {
+          int jj, kk;
+          group_node<N, QJ>(g, j, k, jj, kk);
+          double acc[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            acc[c] = double(rg[g][c]);
+          finish(c0, std::integral_constant<int, decltype(c0)::value + 3>(),
+                 i + Nq * (jj + Nq * kk), i, jj, kk, acc);
+        }
+      };
+      {
+        CT rg[G][3];
+        group_normal<N, QJ, QK, CT>(qv, sD, me, s, i, j, k, rg);
+        group(std::integral_constant<int, 3>(), rg);
+      }
+      // keep the next group's loads below this group's stores (otherwise
+      // the compiler hoists them and spills)
+      asm volatile("" ::: "memory");
+      {
+        CT rg[G][3];
+        group_shear<N, QJ, QK, CT>(qv, sD, me, s, i, j, k, rg);
+        group(std::integral_constant<int, 6>(), rg);
+      }
+      asm volatile("" ::: "memory");
+      {
+        CT rg[G][3];
+        group_velocity<N, QJ, QK, CT>(qv, sD, me, s, i, j, k, rg);
+        group(I0(), rg);
+      }
+    }
+  }
+  else
+  {
+    constexpr int NODE_ITERS = (Np + NT - 1) / NT;
+#pragma unroll 1
+    for (int it = 0; it < NODE_ITERS; ++it)
+    {
+      const int n = node_of_thread<DIM, N, NT>(t + it * NT);
+      if (n >= Np)
+        break;
+      const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
+      double acc[NFLD];
+      if constexpr (!NARROW)
+      {
+        volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
+      }
+      else
+      {
+        CT rv[NFLD];
+        volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
+#pragma unroll
+        for (int c = 0; c < NFLD; ++c)
+          acc[c] = double(rv[c]);
+      }
+      finish(I0(), std::integral_constant<int, NFLD>(), n, i, j, k, acc);
     }
   }
 }
