@@ -134,35 +134,24 @@ template <int DIM, int N> struct Shape
   // and row a of the stress (traction = sg * row a)
   static constexpr int NTF = 2 * DIM;
   static constexpr int ROWS = DIM == 3 ? Nq : 1; // rows of a face
-  // Node-group volume pass (3D, even Nq): a thread owns GQJ x GQK nodes
-  // mirrored in j and k (see group_normal); GROUP_NT threads cover them,
-  // whole warps, 0 where the pass is not used.  3D N=5: node pairs (k,
-  // N-k), 108 threads in four warps.
-  static constexpr int GQJ = 1, GQK = 2;
-  static constexpr int GROUP_NT =
-      0;
   // one thread per node, or per face node where those are fewer (3D N=7:
-  // 384 face nodes, 512 nodes in two passes, so that two CTAs fit an SM),
-  // or the node-group pass's threads
+  // 384 face nodes, 512 nodes in two passes, so that two CTAs fit an SM)
   static constexpr int work =
-      GROUP_NT ? GROUP_NT
-               : ((DIM == 3 && N == 7) ? NF * Nfp
-                                       : (Np > NF * Nfp ? Np : NF * Nfp));
+      (DIM == 3 && N == 7) ? NF * Nfp : (Np > NF * Nfp ? Np : NF * Nfp);
   static constexpr int NT = ((work + 31) / 32) * 32 > 1024
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
   // CTAs per SM the register allocation is sized for (about 96 registers;
-  // 3D N=5: seven CTAs of 128 threads at 72 registers, as many as the
-  // shared memory admits, with dq read from L2)
+  // 3D N=5: four CTAs of 224 threads at 72 registers)
   static constexpr int MINB_RAW = 65536 / (NT * 96);
   static constexpr int MINB = (DIM == 3 && N == 7)
                                   ? 2
                                   : (DIM == 3 && N == 5)
                                         ? 4
                                         : (MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW));
-  // dq read from global memory (L2) in the update instead of staged in
-  // shared memory
-  static constexpr bool DQ_L2 = DIM == 3 && N == 5;
+  // precision form: dq read from global memory (L2) in the update instead
+  // of staged in shared memory
+  static constexpr bool DQ_L2_NARROW = DIM == 3 && N == 5;
   static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
   // shared memory regions in doubles (all even, so 16-byte aligned)
   static constexpr int SM_QS = NFLD * Np + (NFLD * Np) % 2; // q

@@ -78,55 +78,6 @@ __device__ __forceinline__ int node_of_thread(int t)
     return t < Np ? t : Np;
 }
 
-// The node-group volume pass runs where the shape provides it and the CTA
-// (or sub-element) has its thread count.
-template <int DIM, int N, int NT> __host__ __device__ constexpr bool group_pass()
-{
-  return Shape<DIM, N>::GROUP_NT != 0 && NT == Shape<DIM, N>::GROUP_NT;
-}
-
-// Nodes of thread t in the node-group pass: (i, j, k) with j < Nq/2 if
-// paired in j, k < Nq/2 if paired in k.  As in node_of_thread, when a plane
-// of the (i, j) range holds between 32 and 64 of them, warp w takes the
-// first 32 of plane w and the last warp the rest of every plane.  False for
-// threads without nodes.
-template <int DIM, int N, int NT>
-__device__ __forceinline__ bool group_of_thread(int t, int &i, int &j, int &k)
-{
-  using S = Shape<DIM, N>;
-  constexpr int Nq = S::Nq;
-  constexpr int P = (S::GQJ == 2 ? Nq / 2 : Nq) * Nq;
-  constexpr int KP = S::GQK == 2 ? Nq / 2 : Nq;
-  int p, plane;
-  if constexpr (P > 32 && P < 64)
-  {
-    if (t < 32 * KP)
-    {
-      plane = t >> 5;
-      p = t & 31;
-    }
-    else
-    {
-      const int r = t - 32 * KP;
-      if (r >= (P - 32) * KP)
-        return false;
-      plane = r / (P - 32);
-      p = 32 + r % (P - 32);
-    }
-  }
-  else
-  {
-    if (t >= P * KP)
-      return false;
-    plane = t / P;
-    p = t % P;
-  }
-  i = p % Nq;
-  j = p / Nq;
-  k = plane;
-  return true;
-}
-
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
 // aligned).  NBUF element buffers (state, dq, face traces / lifted
 // contributions, face flux constants) let the loads of the next element fly
@@ -159,15 +110,15 @@ __host__ __device__ constexpr int resident_ctas()
   return Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
 }
 
-// dq staged in shared memory unless the shape reads it from L2 in the
-// update (Shape::DQ_L2: prefetched when the element's loads are issued; at
-// four or more resident CTAs per SM the coalesced loads cost fewer L1
-// wavefronts than the bulk copy into shared memory and the reads back), or
-// unless leaving it out admits more resident CTAs (3D N=7 in the precision
-// form: two CTAs instead of one)
+// dq staged in shared memory (TMA) unless the shape reads it from L2 in the
+// update (Shape::DQ_L2_NARROW, the precision form at 3D N=5: prefetched
+// when the element's loads are issued; staging them measured 9 % slower
+// there, while it is 1-2 % faster in the plain form), or unless leaving it
+// out admits more resident CTAs (3D N=7 in the precision form: two CTAs
+// instead of one)
 template <int DIM, int N, typename CT> __host__ __device__ constexpr bool stage_dqs()
 {
-  if (Shape<DIM, N>::DQ_L2)
+  if (Shape<DIM, N>::DQ_L2_NARROW && sizeof(CT) < sizeof(double))
     return false;
   return resident_ctas<DIM, N, CT, 1, true>() >=
          resident_ctas<DIM, N, CT, 1, false>();
@@ -592,14 +543,30 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         atomicExch(d.err, 2);
     }
   }
-  // Finish node n = (i, j, k) for fields [C0, C1), acc[c - C0] holding s
-  // times its volume right-hand side: the lifted jumps of the faces it lies
-  // on (at most one per axis, in face order), the point source, then the
-  // stage update (or the right-hand side out).  Every node pass goes
-  // through here.
-  auto finish = [&](auto c0, auto c1, int n, int i, int j, int k,
-                    double *acc) {
-    constexpr int C0 = decltype(c0)::value, C1 = decltype(c1)::value;
+  constexpr int NODE_ITERS = (Np + NT - 1) / NT;
+#pragma unroll 1
+  for (int it = 0; it < NODE_ITERS; ++it)
+  {
+    const int n = node_of_thread<DIM, N, NT>(t + it * NT);
+    if (n >= Np)
+      break;
+    const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
+    double acc[NFLD];
+    if constexpr (!NARROW)
+    {
+      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
+    }
+    else
+    {
+      CT rv[NFLD];
+      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        acc[c] = double(rv[c]);
+    }
+
+    // lifted jumps of the faces this node lies on (at most one per axis, in
+    // face order)
 #pragma unroll
     for (int ax = 0; ax < DIM; ++ax)
     {
@@ -607,29 +574,28 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       if (idx != 0 && idx != N)
         continue;
       const int side = idx == N;
-      const int f = 2 * ax + side;
       const int pn = DIM == 3 ? (ax == 0 ? j + Nq * k
                                          : (ax == 1 ? i + Nq * k : i + Nq * j))
                               : (ax == 0 ? j : i);
-      const double *jp = pt + f * NTF * Nfp + pn;
+      const double *jp = pt + (2 * ax + side) * NTF * Nfp + pn;
       CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
       for (int c = 0; c < NJ; ++c)
         J[jslot<DIM>(c)] = CT(jp[c * Nfp]);
       lift_face<DIM, CT>(J, ax, side ? CT(1) : CT(-1), lfac[ax], me, lc);
 #pragma unroll
-      for (int c = C0; c < C1; ++c)
-        acc[c - C0] += double(lc[c]);
+      for (int c = 0; c < NFLD; ++c)
+        acc[c] += double(lc[c]);
     }
 
     // point source on the velocity: s f(t_stage) F phi_n(x_s) / (rho w_n J)
-    if (C0 < DIM && e == d.src.elem)
+    if (e == d.src.elem)
     {
       const double ts = d.clock->time + sp.C * d.dt;
       const double g = s * ricker(ts, d.src.f0, d.src.t0) * d.src.w[n] * me.irho;
 #pragma unroll
-      for (int c = C0; c < (C1 < DIM ? C1 : DIM); ++c)
-        acc[c - C0] += g * d.src.force[c];
+      for (int c = 0; c < DIM; ++c)
+        acc[c] += g * d.src.force[c];
     }
 
     if constexpr (MODE != MODE_RHS)
@@ -637,92 +603,21 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       if (rd)
       {
 #pragma unroll
-        for (int c = C0; c < C1; ++c)
-          acc[c - C0] +=
-              a * (DQS ? R[c * Np + n] : d.dq[c * fs + eoff + n]);
+        for (int c = 0; c < NFLD; ++c)
+          acc[c] += a * (DQS ? R[c * Np + n] : d.dq[c * fs + eoff + n]);
       }
 #pragma unroll
-      for (int c = C0; c < C1; ++c)
+      for (int c = 0; c < NFLD; ++c)
       {
-        d.dq[c * fs + eoff + n] = acc[c - C0];
-        d.qout[c * fs + eoff + n] = qs[c * Np + n] + sp.B * acc[c - C0];
+        d.dq[c * fs + eoff + n] = acc[c];
+        d.qout[c * fs + eoff + n] = qs[c * Np + n] + sp.B * acc[c];
       }
     }
     else
     {
 #pragma unroll
-      for (int c = C0; c < C1; ++c)
-        d.rhs[c * fs + eoff + n] = acc[c - C0];
-    }
-  };
-  using I0 = std::integral_constant<int, 0>;
-
-  if constexpr (group_pass<DIM, N, NT>())
-  {
-    // node groups (see group_normal): normal stress, shear stress, velocity
-    constexpr int QJ = S::GQJ, QK = S::GQK, G = QJ * QK;
-    int i, j, k;
-    if (group_of_thread<DIM, N, NT>(t, i, j, k))
-    {
-      auto group = [&](auto c0, const CT (*rg)[3]) {
-#pragma unroll
-        for (int g = 0; g < G; ++g)
-        {
-          int jj, kk;
-          group_node<N, QJ>(g, j, k, jj, kk);
-          double acc[3];
-#pragma unroll
-          for (int c = 0; c < 3; ++c)
-            acc[c] = double(rg[g][c]);
-          finish(c0, std::integral_constant<int, decltype(c0)::value + 3>(),
-                 i + Nq * (jj + Nq * kk), i, jj, kk, acc);
-        }
-      };
-      {
-        CT rg[G][3];
-        group_normal<N, QJ, QK, CT>(qv, sD, me, s, i, j, k, rg);
-        group(std::integral_constant<int, 3>(), rg);
-      }
-      // keep the next group's loads below this group's stores (otherwise
-      // the compiler hoists them and spills)
-      asm volatile("" ::: "memory");
-      {
-        CT rg[G][3];
-        group_shear<N, QJ, QK, CT>(qv, sD, me, s, i, j, k, rg);
-        group(std::integral_constant<int, 6>(), rg);
-      }
-      asm volatile("" ::: "memory");
-      {
-        CT rg[G][3];
-        group_velocity<N, QJ, QK, CT>(qv, sD, me, s, i, j, k, rg);
-        group(I0(), rg);
-      }
-    }
-  }
-  else
-  {
-    constexpr int NODE_ITERS = (Np + NT - 1) / NT;
-#pragma unroll 1
-    for (int it = 0; it < NODE_ITERS; ++it)
-    {
-      const int n = node_of_thread<DIM, N, NT>(t + it * NT);
-      if (n >= Np)
-        break;
-      const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
-      double acc[NFLD];
-      if constexpr (!NARROW)
-      {
-        volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
-      }
-      else
-      {
-        CT rv[NFLD];
-        volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
-#pragma unroll
-        for (int c = 0; c < NFLD; ++c)
-          acc[c] = double(rv[c]);
-      }
-      finish(I0(), std::integral_constant<int, NFLD>(), n, i, j, k, acc);
+      for (int c = 0; c < NFLD; ++c)
+        d.rhs[c * fs + eoff + n] = acc[c];
     }
   }
 }
