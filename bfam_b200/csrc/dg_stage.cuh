@@ -78,6 +78,18 @@ __device__ __forceinline__ int node_of_thread(int t)
     return t < Np ? t : Np;
 }
 
+// A face node's flux jump in its trace slot (one double): stored at the
+// precision of the right-hand side (a float in the slot's first four bytes
+// in the precision form), so that it is never widened and narrowed again.
+template <typename CT> __device__ __forceinline__ void put_jump(double *slot, CT v)
+{
+  *reinterpret_cast<CT *>(slot) = v;
+}
+template <typename CT> __device__ __forceinline__ CT get_jump(const double *slot)
+{
+  return *reinterpret_cast<const CT *>(slot);
+}
+
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
 // aligned).  NBUF element buffers (state, dq, face traces / lifted
 // contributions, face flux constants) let the loads of the next element fly
@@ -221,11 +233,14 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
     if (t == 0)
     {
       fence_proxy_async(); // shared memory of the previous element is free
-      mbar_expect_tx(bar_q, NFLD * Np * sizeof(double));
+      mbar_expect_tx(bar_q, NFLD * Np * sizeof(double) + NF * sizeof(double4));
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
         bulk_g2s(qs + c * Np, d.qin + c * fs + eoff, Np * sizeof(double),
                  bar_q);
+      // the face flux constants with the state, so that no thread needs
+      // another thread's copies before the face phase
+      bulk_g2s(fcf, d.fcE + (size_t)e * NF, NF * sizeof(double4), bar_q);
       if (rd)
       {
         if constexpr (stage_dqs<DIM, N, CT>())
@@ -275,7 +290,7 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
       for (int c = 0; c < NTF; ++c)
         cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
     }
-    if (pn == 0)
+    if (!S::TMA && pn == 0)
     {
       const double *fc =
           reinterpret_cast<const double *>(d.fcE + (size_t)e * NF + f);
@@ -283,7 +298,7 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
       cp_async16(fcf + 4 * f + 2, fc + 2);
     }
   }
-  cp_async_commit(); // own state (non-TMA path), face traces, constants
+  cp_async_commit(); // own state and constants (non-TMA path), face traces
 
 }
 
@@ -393,10 +408,18 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
     Sub<NT, EPC>::sync(); // other threads' cp.async writes of q
   if constexpr (NARROW)
   {
-    for (int w = t; w < NFLD * Np; w += NT)
-      qv[w] = CT(qs[w] - qs[(w / Np) * Np]);
+    for (int n = t; n < Np; n += NT)
+    {
+#pragma unroll
+      for (int c = 0; c < NFLD; ++c)
+        qv[c * Np + n] = CT(qs[c * Np + n] - qs[c * Np]);
+    }
   }
-  Sub<NT, EPC>::sync();
+  // With the state and flux constants by TMA, a thread's face pass reads
+  // only its own gathered trace slots (its own cp.async group), so only the
+  // fine-side interpolation, which reads whole lines, needs the barrier.
+  if (!S::TMA || nfine)
+    Sub<NT, EPC>::sync();
   // lift factor of face axis ax: s (2/h_ax) / w_0
   CT lfac[3];
 #pragma unroll
@@ -475,7 +498,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         }
 #pragma unroll
         for (int c = 0; c < NJ; ++c)
-          x[c * Nfp + pp] = double(J[jslot<DIM>(c)]);
+          put_jump<CT>(x + c * Nfp + pp, J[jslot<DIM>(c)]);
       }
     }
   }
@@ -493,7 +516,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
 #pragma unroll
       for (int p = 0; p < NPC; ++p)
         sum += mb[(p * NJ + c) * Nfp];
-      pt[(f * NTF + c) * Nfp + pn] = double(CT(sum));
+      put_jump<CT>(pt + (f * NTF + c) * Nfp + pn, CT(sum));
     }
   }
 
@@ -551,22 +574,11 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
     if (n >= Np)
       break;
     const int i = n % Nq, j = (n / Nq) % Nq, k = n / (Nq * Nq);
-    double acc[NFLD];
-    if constexpr (!NARROW)
-    {
-      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, acc);
-    }
-    else
-    {
-      CT rv[NFLD];
-      volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
-#pragma unroll
-      for (int c = 0; c < NFLD; ++c)
-        acc[c] = double(rv[c]);
-    }
-
-    // lifted jumps of the faces this node lies on (at most one per axis, in
-    // face order)
+    // s times the right-hand side in CT: the volume term, then the lifted
+    // jumps of the faces this node lies on (at most one per axis, in face
+    // order); widened to FP64 once for the update
+    CT rv[NFLD];
+    volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
 #pragma unroll
     for (int ax = 0; ax < DIM; ++ax)
     {
@@ -581,12 +593,16 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
       for (int c = 0; c < NJ; ++c)
-        J[jslot<DIM>(c)] = CT(jp[c * Nfp]);
+        J[jslot<DIM>(c)] = get_jump<CT>(jp + c * Nfp);
       lift_face<DIM, CT>(J, ax, side ? CT(1) : CT(-1), lfac[ax], me, lc);
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
-        acc[c] += double(lc[c]);
+        rv[c] += lc[c];
     }
+    double acc[NFLD];
+#pragma unroll
+    for (int c = 0; c < NFLD; ++c)
+      acc[c] = double(rv[c]);
 
     // point source on the velocity: s f(t_stage) F phi_n(x_s) / (rho w_n J)
     if (e == d.src.elem)
