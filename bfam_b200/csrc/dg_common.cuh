@@ -141,14 +141,15 @@ template <int DIM, int N> struct Shape
   static constexpr int NT = ((work + 31) / 32) * 32 > 1024
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
-  // CTAs per SM the register allocation is sized for (about 96 registers;
-  // 3D N=5: four CTAs of 224 threads at 72 registers)
+  // CTAs per SM the register allocation is sized for (about 96 registers,
+  // at most 16 CTAs of the smallest shapes; 3D N=5: four CTAs of 224
+  // threads at 72 registers)
   static constexpr int MINB_RAW = 65536 / (NT * 96);
   static constexpr int MINB = (DIM == 3 && N == 7)
                                   ? 2
                                   : (DIM == 3 && N == 5)
                                         ? 4
-                                        : (MINB_RAW < 1 ? 1 : (MINB_RAW > 8 ? 8 : MINB_RAW));
+                                        : (MINB_RAW < 1 ? 1 : (MINB_RAW > 16 ? 16 : MINB_RAW));
   // precision form: dq read from global memory (L2) in the update instead
   // of staged in shared memory
   static constexpr bool DQ_L2_NARROW = DIM == 3 && N == 5;

@@ -136,17 +136,21 @@ template <int DIM, int N, typename CT> __host__ __device__ constexpr bool stage_
          resident_ctas<DIM, N, CT, 1, false>();
 }
 
-// Two buffers (loads of the next element overlap the current one) unless
-// they cost resident CTAs, which hide latency better (e.g. N = 5: three
-// CTAs of 7 warps with one buffer, two with two).
+// Two buffers (a persistent grid; the loads of the next element overlap the
+// current one) only where one buffer leaves fewer than four resident CTAs
+// per SM and the second buffer costs none.  With four or more one-element
+// CTAs per SM the block scheduler's balancing of the uneven element costs
+// wins (3D N=3: 105.8 vs 91.5 G DOF-updates/s, N=4: 83.7 vs 72.0, 2D N=3:
+// 54.0 vs 51.3; 3D N=2: 57.5 vs 61.0 in FP64 but 66.6 vs 59.2 in the
+// precision form; 2D N=5: 61.8 vs 70.5), and a second buffer that costs
+// resident CTAs loses (N=5: three CTAs of 7 warps with one buffer, two with
+// two).
 template <int DIM, int N, typename CT> __host__ __device__ constexpr int nbuf()
 {
   constexpr bool DQS = stage_dqs<DIM, N, CT>();
-  return resident_ctas<DIM, N, CT, 2, DQS>() >=
-                     resident_ctas<DIM, N, CT, 1, DQS>() &&
-                 resident_ctas<DIM, N, CT, 2, DQS>() > 0
-             ? 2
-             : 1;
+  constexpr int one = resident_ctas<DIM, N, CT, 1, DQS>(),
+                two = resident_ctas<DIM, N, CT, 2, DQS>();
+  return one < 4 && two >= one && two > 0 ? 2 : 1;
 }
 
 // Elements per CTA: a CTA of EPC * NT threads holds EPC sub-elements of NT
