@@ -872,19 +872,24 @@ def main():
         host_np[...] = p.q0
         out = torch.empty_like(host, pin_memory=True).numpy()
         tsolve = bf.LSRK(dom)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         torch.cuda.synchronize()
-        e0.record(stream)
+        ev[0].record(stream)
         dom.set_fields(host_np)
+        ev[1].record(stream)
         tsolve.step(p.dt, p.nsteps, use_graph=use_graph)
+        ev[2].record(stream)
         dom.get_fields(out)
-        e1.record(stream)
-        e1.synchronize()
-        el = e0.elapsed_time(e1) / 1e3
+        ev[3].record(stream)
+        ev[3].synchronize()
+        el = ev[0].elapsed_time(ev[3]) / 1e3
+        phases = {k: ev[i].elapsed_time(ev[i + 1]) / 1e3
+                  for i, k in enumerate(("upload_s", "steps_s", "download_s"))}
         el = max_over_ranks(el, local)
         nbytes = host_np.nbytes
         e2e = {"value": p.ndof * ns * p.nsteps * ws / el, "unit": "DOF-updates/s",
+               "phases": phases,
+               "steps_only_value": p.ndof * ns * p.nsteps / phases["steps_s"],
                "h2d_bytes_per_step": nbytes / p.nsteps,
                "d2h_bytes_per_step": nbytes / p.nsteps,
                "h2d_bytes_per_solve": nbytes, "d2h_bytes_per_solve": nbytes,

@@ -142,14 +142,18 @@ template <int DIM, int N> struct Shape
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
   // CTAs per SM the register allocation is sized for (about 96 registers,
-  // at most 16 CTAs of the smallest shapes; 3D N=5: four CTAs of 224
-  // threads at 72 registers)
+  // at most 16 CTAs of the smallest shapes; 3D N=5: five CTAs of 224
+  // threads at 56 registers in the plain form, which then reads dq from L2
+  // for room in shared memory (121.8-123.6 vs 120.0-120.5 G DOF-updates/s
+  // with four CTAs at 72 registers and dq staged), four in the precision
+  // form (126.3 vs 113.6 with five: its conversions need the registers))
   static constexpr int MINB_RAW = 65536 / (NT * 96);
   static constexpr int MINB = (DIM == 3 && N == 7)
                                   ? 2
                                   : (DIM == 3 && N == 5)
-                                        ? 4
+                                        ? 5
                                         : (MINB_RAW < 1 ? 1 : (MINB_RAW > 16 ? 16 : MINB_RAW));
+  static constexpr int MINB_NARROW = (DIM == 3 && N == 5) ? 4 : MINB;
   // precision form: dq read from global memory (L2) in the update instead
   // of staged in shared memory
   static constexpr bool DQ_L2_NARROW = DIM == 3 && N == 5;

@@ -112,6 +112,13 @@ template <int DIM, int N, typename CT, int NBUF, bool DQS = true> struct Tile
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(double);
 };
 
+// the shape's register budget in resident CTAs per SM for arithmetic CT
+template <int DIM, int N, typename CT> __host__ __device__ constexpr int shape_minb()
+{
+  return sizeof(CT) < sizeof(double) ? Shape<DIM, N>::MINB_NARROW
+                                     : Shape<DIM, N>::MINB;
+}
+
 // CTAs per SM that the shape's register budget and NBUF buffers admit
 // (228 KB of shared memory per SM, 1 KB reserved per CTA)
 template <int DIM, int N, typename CT, int NBUF, bool DQS = true>
@@ -119,15 +126,16 @@ __host__ __device__ constexpr int resident_ctas()
 {
   constexpr size_t bytes = Tile<DIM, N, CT, NBUF, DQS>::BYTES;
   constexpr int by_smem = bytes > 227 * 1024 ? 0 : (int)(233472 / (bytes + 1024));
-  return Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
+  constexpr int m = shape_minb<DIM, N, CT>();
+  return m < by_smem ? m : by_smem;
 }
 
 // dq staged in shared memory (TMA) unless the shape reads it from L2 in the
 // update (Shape::DQ_L2_NARROW, the precision form at 3D N=5: prefetched
 // when the element's loads are issued; staging them measured 9 % slower
-// there, while it is 1-2 % faster in the plain form), or unless leaving it
-// out admits more resident CTAs (3D N=7 in the precision form: two CTAs
-// instead of one)
+// there), or unless leaving it out admits more resident CTAs (the plain
+// form at 3D N=5: five CTAs instead of four; 3D N=7 in the precision form:
+// two instead of one)
 template <int DIM, int N, typename CT> __host__ __device__ constexpr bool stage_dqs()
 {
   if (Shape<DIM, N>::DQ_L2_NARROW && sizeof(CT) < sizeof(double))
@@ -781,7 +789,7 @@ template <int DIM, int N, typename CT>
 __host__ __device__ constexpr int stage_min_ctas()
 {
   constexpr int by_smem = (int)(233472 / (stage_smem_bytes<DIM, N, CT>() + 1024));
-  constexpr int m = Shape<DIM, N>::MINB < by_smem ? Shape<DIM, N>::MINB : by_smem;
+  constexpr int m = shape_minb<DIM, N, CT>() < by_smem ? shape_minb<DIM, N, CT>() : by_smem;
   return m < 1 ? 1 : m;
 }
 
