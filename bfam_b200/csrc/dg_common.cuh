@@ -142,18 +142,26 @@ template <int DIM, int N> struct Shape
                                 ? 1024
                                 : ((work + 31) / 32) * 32;
   // CTAs per SM the register allocation is sized for (about 96 registers,
-  // at most 16 CTAs of the smallest shapes; 3D N=5: five CTAs of 224
-  // threads at 56 registers in the plain form, which then reads dq from L2
-  // for room in shared memory (121.8-123.6 vs 120.0-120.5 G DOF-updates/s
-  // with four CTAs at 72 registers and dq staged), four in the precision
-  // form (126.3 vs 113.6 with five: its conversions need the registers))
+  // at most 16 CTAs of the smallest shapes), measured where it matters
+  // (G DOF-updates/s, same box):
+  //   3D N=5: five CTAs of 224 threads at 56 registers in the plain form,
+  //     which then reads dq from L2 for room in shared memory (121.8-123.6
+  //     vs 120.0-120.5 with four CTAs at 72 registers and dq staged); four
+  //     in the precision form (126.3 vs 113.6 with five);
+  //   3D N=3: ten CTAs of 96 threads at 64 registers in the plain form
+  //     (109.1-109.4 vs 105.1-105.3 with seven; 105.6 with twelve), twelve
+  //     in the precision form, which then reads dq from L2 (115.4 vs 104.3
+  //     with seven, 109.2 with ten);
+  //   3D N=7: two CTAs of 384 threads (three: 92.2 vs 102.3, spills).
   static constexpr int MINB_RAW = 65536 / (NT * 96);
-  static constexpr int MINB = (DIM == 3 && N == 7)
-                                  ? 2
-                                  : (DIM == 3 && N == 5)
-                                        ? 5
-                                        : (MINB_RAW < 1 ? 1 : (MINB_RAW > 16 ? 16 : MINB_RAW));
-  static constexpr int MINB_NARROW = (DIM == 3 && N == 5) ? 4 : MINB;
+  static constexpr int MINB =
+      (DIM == 3 && N == 7)   ? 2
+      : (DIM == 3 && N == 5) ? 5
+      : (DIM == 3 && N == 3) ? 10
+                             : (MINB_RAW < 1 ? 1 : (MINB_RAW > 16 ? 16 : MINB_RAW));
+  static constexpr int MINB_NARROW = (DIM == 3 && N == 5)   ? 4
+                                     : (DIM == 3 && N == 3) ? 12
+                                                            : MINB;
   // precision form: dq read from global memory (L2) in the update instead
   // of staged in shared memory
   static constexpr bool DQ_L2_NARROW = DIM == 3 && N == 5;
