@@ -162,8 +162,11 @@ template <int DIM, int N> struct Shape
   static constexpr int MINB_NARROW = (DIM == 3 && N == 5)   ? 4
                                      : (DIM == 3 && N == 3) ? 12
                                                             : MINB;
-  // precision form: dq read from global memory (L2) in the update instead
-  // of staged in shared memory
+  // dq read from global memory (L2) in the update instead of staged in
+  // shared memory: at 3D N=7 (two CTAs of 103 KB with dq staged leave the
+  // L1 cache about 22 KB for the neighbour-trace gathers; 105.6 vs 102.4 G
+  // DOF-updates/s in the plain form), and in the precision form at N=5
+  static constexpr bool DQ_L2 = DIM == 3 && N == 7;
   static constexpr bool DQ_L2_NARROW = DIM == 3 && N == 5;
   static constexpr bool TMA = (Np % 2) == 0; // 16-byte aligned element rows
   // shared memory regions in doubles (all even, so 16-byte aligned)

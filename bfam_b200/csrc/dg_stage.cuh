@@ -131,14 +131,14 @@ __host__ __device__ constexpr int resident_ctas()
 }
 
 // dq staged in shared memory (TMA) unless the shape reads it from L2 in the
-// update (Shape::DQ_L2_NARROW, the precision form at 3D N=5: prefetched
-// when the element's loads are issued; staging them measured 9 % slower
-// there), or unless leaving it out admits more resident CTAs (the plain
-// form at 3D N=5: five CTAs instead of four; 3D N=7 in the precision form:
-// two instead of one)
+// update (Shape::DQ_L2 / DQ_L2_NARROW: 3D N=7, and the precision form at
+// 3D N=5, where staging measured 9 % slower; the rows are prefetched into
+// L2 when the element's loads are issued), or unless leaving it out admits
+// more resident CTAs (the plain form at 3D N=5: five CTAs instead of four)
 template <int DIM, int N, typename CT> __host__ __device__ constexpr bool stage_dqs()
 {
-  if (Shape<DIM, N>::DQ_L2_NARROW && sizeof(CT) < sizeof(double))
+  if (Shape<DIM, N>::DQ_L2 ||
+      (Shape<DIM, N>::DQ_L2_NARROW && sizeof(CT) < sizeof(double)))
     return false;
   return resident_ctas<DIM, N, CT, 1, true>() >=
          resident_ctas<DIM, N, CT, 1, false>();
