@@ -52,6 +52,8 @@ def parse():
                     help="cfg4: Poisson arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=200, help="cfg4: requests per rate")
     ap.add_argument("--chunk", type=int, default=25, help="cfg4: steps per batch chunk")
+    ap.add_argument("--chunk-s", type=float, default=0.1,
+                    help="cfg4: seconds per batch chunk at most (0: steps only)")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="arithmetic of the right-hand side (default: fp64; cfg3, cfg4: "
                          "fp32); with cfg2 it times that one form only, as cfg1 does")
@@ -612,7 +614,8 @@ def run_serving(args):
         for rate in [float(x) for x in args.rates.split(",")]:
             reqs = serving.poisson_requests(rate, args.requests, seed=2)
             srv = serving.Server(serving.GpuEngine(prec, device=local),
-                                 budget_bytes=150 * 10 ** 9, chunk=args.chunk)
+                                 budget_bytes=150 * 10 ** 9, chunk=args.chunk,
+                                 max_chunk_s=args.chunk_s or None)
             stats = srv.run(reqs, realtime=True)
             s = stats.summary()
             s["rate_per_s"] = rate

@@ -248,13 +248,19 @@ class Server:
     """Continuous-batching request loop (see the module docstring)."""
 
     def __init__(self, engine, budget_bytes: int = 150 * 10 ** 9, max_active: int = 1024,
-                 chunk: int = 25, clock=time.perf_counter, sleep=time.sleep):
+                 chunk: int = 25, clock=time.perf_counter, sleep=time.sleep,
+                 max_chunk_s: float | None = None):
+        """`chunk`: steps per chunk at most; `max_chunk_s`: if set, a chunk is
+        also cut to about that many seconds, from the time per DOF-update of
+        the chunks so far (a request admitted during a chunk waits for its
+        end, so long chunks of a heavily loaded batch delay every newcomer)."""
         self.engine = engine
         self.budget = budget_bytes
         self.max_active = max_active
         self.chunk = chunk
         self.clock = clock
         self.sleep = sleep
+        self.max_chunk_s = max_chunk_s
 
     def run(self, requests: list[Request], realtime: bool = True) -> ServeStats:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
@@ -266,6 +272,8 @@ class Server:
         chunks = 0
         dof_updates = 0
         in_flight = 0      # steps of the chunk on the device
+        chunk_t0 = 0.0     # when the chunk in flight was issued
+        spd = None         # seconds per DOF-update of the chunks so far
         t_start = self.clock()
         now = lambda: self.clock() - t_start  # noqa: E731
         for r in requests:
@@ -275,6 +283,10 @@ class Server:
             # the chunk in flight ends: retire finished requests
             if in_flight:
                 self.engine.wait()
+                work = sum(r.dofs for r, _, _ in active) * 5 * in_flight
+                if work > 0:
+                    s_chunk = (self.clock() - chunk_t0) / work
+                    spd = s_chunk if spd is None else 0.5 * (spd + s_chunk)
                 chunks += 1
                 keep = []
                 for r, d, dt in active:
@@ -300,6 +312,10 @@ class Server:
             max_act = max(max_act, len(active))
             if active:
                 c = min(self.chunk, min(r.nsteps - r.steps_done for r, _, _ in active))
+                if self.max_chunk_s and spd:
+                    step_s = sum(r.dofs for r, _, _ in active) * 5 * spd
+                    c = max(1, min(c, int(self.max_chunk_s / step_s)))
+                chunk_t0 = self.clock()
                 rb0 = getattr(self.engine, "rebuilds", 0)
                 self.engine.step([d for _, d, _ in active], [dt for _, _, dt in active],
                                  [r.time for r, _, _ in active], c)

@@ -139,3 +139,41 @@ def test_next_chunk_is_queued_before_new_arrivals_are_set_up():
             nxt = next((x for x in eng.log[i + 1:] if x != "wait"), None)
             assert nxt in ("step", None), eng.log[i:i + 4]
     assert eng.log.count("create") == len(reqs)
+
+
+def test_chunks_are_cut_to_the_time_bound():
+    """with max_chunk_s a chunk is cut to about that many seconds of work
+    (estimated from the chunks so far), so a request admitted during a chunk
+    joins within about max_chunk_s; without it chunks run the full step
+    count"""
+    rate = 2e10  # DOF-updates per second of the stand-in device
+
+    def run(max_chunk_s):
+        t = [0.0]
+        work = []
+
+        class Timed(FakeEngine):
+            def step(self, doms, dts, times, chunk):
+                super().step(doms, dts, times, chunk)
+                w = sum(self.live[id(d)].dofs for d in doms) * 5
+                work.append((w * chunk / rate, w / rate))
+                t[0] += w * chunk / rate  # the host waits for it in wait()
+
+        reqs = serving.poisson_requests(50.0, 30, seed=7, n_range=(8, 12),
+                                        steps_range=(60, 120))
+        eng = Timed()
+        srv = serving.Server(eng, chunk=50, clock=lambda: t[0],
+                             sleep=lambda s: None, max_chunk_s=max_chunk_s)
+        srv.run(reqs, realtime=False)
+        for r in reqs:
+            assert r.steps_done == r.nsteps and r.finished is not None
+        return work
+
+    full = run(None)
+    cut = run(0.05)
+    assert max(s for s, _ in full) > 0.1
+    # after the first chunk (whose time is not known yet) every chunk is at
+    # most the bound, or a single step where one step exceeds it
+    for chunk_s, step_s in cut[1:]:
+        assert chunk_s <= 0.05 + 1e-12 or abs(chunk_s - step_s) < 1e-12
+    assert len(cut) > len(full)
