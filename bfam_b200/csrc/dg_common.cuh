@@ -422,96 +422,46 @@ __device__ __forceinline__ void apply_half_s(const AT *A, int top, const T *v,
     out[m] = top ? o[N - m] : o[m];
 }
 
-// One line of Nq doubles of a face array in shared memory, x[STRIDE i]:
-// a line along face axis 0 (STRIDE 1) is read and written as 16-byte pairs
-// where Nq is even.  Lanes own lines Nq doubles apart, an even number of
-// 8-byte words, so 8-byte accesses would use only half of the bank pairs
-// (two-way conflicts); 16-byte ones are conflict-free in each quarter-warp
-// phase and take half the instructions.
-template <int N, int STRIDE>
-__device__ __forceinline__ void line_load(const double *x, double *v)
-{
-  constexpr int Nq = N + 1;
-  if constexpr (STRIDE == 1 && Nq % 2 == 0)
-  {
-#pragma unroll
-    for (int i = 0; i < Nq; i += 2)
-    {
-      const double2 p = *reinterpret_cast<const double2 *>(x + i);
-      v[i] = p.x;
-      v[i + 1] = p.y;
-    }
-  }
-  else
-  {
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-      v[i] = x[STRIDE * i];
-  }
-}
-template <int N, int STRIDE>
-__device__ __forceinline__ void line_store(double *x, const double *v)
-{
-  constexpr int Nq = N + 1;
-  if constexpr (STRIDE == 1 && Nq % 2 == 0)
-  {
-#pragma unroll
-    for (int i = 0; i < Nq; i += 2)
-      *reinterpret_cast<double2 *>(x + i) = make_double2(v[i], v[i + 1]);
-  }
-  else
-  {
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-      x[STRIDE * i] = v[i];
-  }
-}
-
 // line_apply with the operator in shared memory (OFFSET: interpolate the
 // variation along the line, as line_apply does for narrow types)
-template <int N, int STRIDE, bool OFFSET, typename T, typename AT>
-__device__ __forceinline__ void line_apply_s(const AT *A, int top, double *x)
+template <int N, bool OFFSET, typename T, typename AT>
+__device__ __forceinline__ void line_apply_s(const AT *A, int top, double *x,
+                                             int stride)
 {
   constexpr int Nq = N + 1;
-  double xd[Nq];
-  line_load<N, STRIDE>(x, xd);
-  const double ref = OFFSET ? xd[0] : 0.0;
+  const double ref = OFFSET ? x[0] : 0.0;
   T v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
-    v[i] = OFFSET ? T(xd[i] - ref) : T(xd[i]);
+    v[i] = OFFSET ? T(x[i * stride] - ref) : T(x[i * stride]);
   apply_half_s<N, T, AT>(A, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    xd[m] = OFFSET ? ref + double(v[m]) : double(v[m]);
-  line_store<N, STRIDE>(x, xd);
+    x[m * stride] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
 // In-place 1-D mortar operator pass on one line of a face array
-// x[m0 + Nq*m1] (STRIDE 1: along face axis 0, STRIDE Nq: along axis 1),
+// x[m0 + Nq*m1] (stride 1: along face axis 0, stride Nq: along axis 1),
 // computed in T and stored back in double.  One thread owns one line.  An
 // interpolation in a type narrower than double is applied to the line minus
 // its first value, which is added back in double (interpolation reproduces
 // constants), so that the rounding is relative to the variation along the
 // line rather than to the values.
-template <int N, int STRIDE, bool PROJ, typename T, typename CT>
+template <int N, bool PROJ, typename T, typename CT>
 __device__ __forceinline__ void line_apply(const DiffOp<N, CT> &op, int top,
-                                           double *x)
+                                           double *x, int stride)
 {
   constexpr int Nq = N + 1;
   constexpr bool OFFSET = !PROJ && sizeof(T) < sizeof(double);
-  double xd[Nq];
-  line_load<N, STRIDE>(x, xd);
-  const double ref = OFFSET ? xd[0] : 0.0;
+  const double ref = OFFSET ? x[0] : 0.0;
   T v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
-    v[i] = OFFSET ? T(xd[i] - ref) : T(xd[i]);
+    v[i] = OFFSET ? T(x[i * stride] - ref) : T(x[i * stride]);
   apply_half<N, PROJ, T, CT>(op, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    xd[m] = OFFSET ? ref + double(v[m]) : double(v[m]);
-  line_store<N, STRIDE>(x, xd);
+    x[m * stride] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
 // Field of trace slot c on a face normal to axis ax: slots [0, DIM) are the

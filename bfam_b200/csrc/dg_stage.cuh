@@ -453,9 +453,9 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
         double *x = pt + (f * NTF + c) * Nfp;
         if (pass == 0)
-          line_apply<N, 1, false, CT, CT>(dop, half, x + Nq * line);
+          line_apply<N, false, CT, CT>(dop, half, x + Nq * line, 1);
         else
-          line_apply<N, Nq, false, CT, CT>(dop, half, x + line);
+          line_apply<N, false, CT, CT>(dop, half, x + line, Nq);
       }
       Sub<NT, EPC>::sync();
     }
@@ -542,8 +542,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       const int fr = w / (NJ * ROWS), r = w % (NJ * ROWS);
       const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
       const int c = r / ROWS, line = r % ROWS;
-      line_apply_s<N, 1, false, double, double>(
-          sPb, (hp - 1) & 1, mj + (fr * NJ + c) * Nfp + Nq * line);
+      line_apply_s<N, false, double, double>(
+          sPb, (hp - 1) & 1, mj + (fr * NJ + c) * Nfp + Nq * line, 1);
     }
     Sub<NT, EPC>::sync();
     if (DIM == 3)
@@ -553,8 +553,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int fr = w / (NJ * Nq), r = w % (NJ * Nq);
         const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
         const int c = r / Nq, col = r % Nq;
-        line_apply_s<N, Nq, false, double, double>(
-            sPb, (hp - 1) >> 1, mj + (fr * NJ + c) * Nfp + col);
+        line_apply_s<N, false, double, double>(
+            sPb, (hp - 1) >> 1, mj + (fr * NJ + c) * Nfp + col, Nq);
       }
       Sub<NT, EPC>::sync();
     }
