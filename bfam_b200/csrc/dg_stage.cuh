@@ -3,16 +3,18 @@
 //
 // One element per CTA iteration does:
 //   issue   : every global read of the element is issued up front -- its own
-//             q and dq by TMA bulk copies into shared memory, the neighbours'
-//             face traces by 8-byte cp.async gathers straight into shared
-//             memory, addressed from a per-face descriptor.  This is the
+//             q (and dq, where the shape stages it; else an L2 prefetch of
+//             it) and its faces' flux constants by TMA bulk copies into
+//             shared memory, the neighbours' face traces by 8-byte cp.async
+//             gathers straight into shared memory, addressed from a
+//             per-face descriptor.  This is the
 //             on-device replacement of vmapP and of the bfam_communicator
 //             ghost exchange (src/bfam.c:6783-6877, 2418-2679).  Only the six
 //             trace fields the flux uses are gathered (velocity and the stress
 //             row of the face normal);
 //   face    : upwind flux on the gathered traces (conforming faces and the
-//             fine side of hanging faces), lifted with the lumped LGL mass to
-//             per-node field contributions;
+//             fine side of hanging faces): six jumps per face node, stored
+//             in place of its trace;
 //   mortar  : faces that go through the glue grid (2:1 hanging faces,
 //             src/bfam.c:7328-7520).  The fine element interpolates the coarse
 //             neighbour's trace to its mortar piece (interpolation[1..2]) and
@@ -21,11 +23,11 @@
 //             the coarse face (projection[1..2]) and stores them in a mortar
 //             buffer slot.  The coarse element, launched after its fine
 //             neighbours (elements are launched by level), sums its pieces'
-//             projected jumps and lifts them;
+//             projected jumps;
 //   volume  : one thread per node, the tensor-product LGL derivative along each
 //             axis (the BFAM_KRON_IXIXA / IXAXI / AXIXI contractions of
-//             src/bfam.c:3519-3624 at one node), plus the node's face
-//             contributions;
+//             src/bfam.c:3519-3624 at one node), plus the jumps of the faces
+//             the node lies on, lifted with the lumped LGL mass;
 //   update  : the 2N-storage LSRK stage dq = A dq + dt rhs, q' = q + B dq
 //             (bfamo_lsrk_t, src/bfam.h:1840-1846) in FP64, writing the new
 //             state to the other state buffer so that every element's
@@ -36,7 +38,8 @@
 // right-hand side only) and CT, the arithmetic of the right-hand side (double
 // for the plain form; float for the precision form, where the volume
 // derivative, flux, lift and mortar interpolation run in FP32 while the state,
-// dq, the mortar L2 projection and the update stay FP64).
+// dq, the mortar L2 projection and the update stay FP64; the face jumps and
+// lifts stay FP32 until one widening per field).
 //
 // State layout in HBM: field-major, element, node (bfam's per-field arrays
 // stacked): q[f * K * Np + e * Np + n], n = i + Nq (j + Nq k).
@@ -91,8 +94,8 @@ template <typename CT> __device__ __forceinline__ CT get_jump(const double *slot
 }
 
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
-// aligned).  NBUF element buffers (state, dq, face traces / lifted
-// contributions, face flux constants) let the loads of the next element fly
+// aligned).  NBUF element buffers (state, dq, face traces / flux jumps, face
+// flux constants) let the loads of the next element fly
 // while the current one is computed; the mortar scratch, the 1-D operators,
 // the mbarriers (q and dq per buffer) and the precision form's FP32 tile are
 // single.
@@ -464,8 +467,9 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   // flux on conforming and fine-side faces: the face node's jumps (T* - T-,
   // v* - v-), written in place over the node's own trace slots (a thread
   // reads only its own node's slots: partners' face nodes are in the same
-  // order on aligned trees) and lifted by the node pass.  On a fine face the coarse side's jumps follow from the same Riemann
-  // solution (star state v*, S* n shared by both sides, coarse normal -n):
+  // order on aligned trees) and lifted by the node pass.  On a fine face
+  // the coarse side's jumps follow from the same Riemann solution (star
+  // state v*, S* n shared by both sides, coarse normal -n):
   //   coarse (T* - T-) = -(fine J_T) + [T],  coarse (v* - v-) = fine J_v - [v]
   // with [.] = coarse - fine as seen from the fine side; they go to mj in the
   // coarse piece's node order.
