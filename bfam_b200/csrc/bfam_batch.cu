@@ -41,6 +41,10 @@ struct BatchTile
   int NT = 0, MINB = 0, NBUF = 1;
   int EPC = 1; // elements per CTA (NT threads each)
   batch_launch_fn launch = nullptr;
+  // the same tile compiled without the coarse-face pass, for launches
+  // whose elements have no coarse-side hanging face (level 0 of domains
+  // without faces glued to another order)
+  batch_launch_fn launch_nc = nullptr;
   batch_prepare_fn prepare = nullptr;
   batch_occupancy_fn occupancy = nullptr;
 };
@@ -51,6 +55,8 @@ struct TileImpl
   static constexpr int NB = EPC == 1 ? nbuf<DIM, N, CT>() : 1;
   static constexpr auto kernel =
       dg_stage_batch_kernel<DIM, N, NT, MINB, MODE_STAGE, CT, NB, EPC>;
+  static constexpr auto kernel_nc =
+      dg_stage_batch_kernel<DIM, N, NT, MINB, MODE_STAGE_NC, CT, NB, EPC>;
   static constexpr size_t SMEM = stage_smem_bytes<DIM, N, CT, EPC>();
   static void launch(const DomainView *v, const int2 *w, int nwork,
                      const StageParams &sp, const double *hops, int grid,
@@ -59,9 +65,21 @@ struct TileImpl
     const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
     kernel<<<grid, NT * EPC, SMEM, st>>>(v, w, nwork, sp, dop);
   }
+  static void launch_nc(const DomainView *v, const int2 *w, int nwork,
+                        const StageParams &sp, const double *hops, int grid,
+                        cudaStream_t st)
+  {
+    const DiffOp<N, CT> dop = make_diffop<N, CT>(hops);
+    kernel_nc<<<grid, NT * EPC, SMEM, st>>>(v, w, nwork, sp, dop);
+  }
   static cudaError_t prepare()
   {
-    return cudaFuncSetAttribute((const void *)kernel,
+    cudaError_t e = cudaFuncSetAttribute(
+        (const void *)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)SMEM);
+    if (e != cudaSuccess)
+      return e;
+    return cudaFuncSetAttribute((const void *)kernel_nc,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)SMEM);
   }
@@ -84,6 +102,7 @@ struct TileImpl
     t.EPC = EPC;
     t.NBUF = NB;
     t.launch = launch;
+    t.launch_nc = launch_nc;
     t.prepare = prepare;
     t.occupancy = occupancy;
     return t;
@@ -93,7 +112,9 @@ struct TileImpl
 // Tile shapes per order.  Tile 0 is the single-domain kernel's shape (its
 // register budget sized for the CTAs the shared memory admits); the others
 // trade registers for resident CTAs or threads for nodes per thread (N = 7:
-// 384 threads, one per face node, over 512 nodes).
+// 384 threads, one per face node, over 512 nodes).  At N = 5 the batch
+// kernel, which reads its domain views and work items from memory, spills
+// at tile 0's five CTAs in FP64; the four-CTA tile beside it does not.
 template <typename CT> std::vector<BatchTile> tiles_for(int dim, int N)
 {
   std::vector<BatchTile> v;
@@ -115,8 +136,8 @@ template <typename CT> std::vector<BatchTile> tiles_for(int dim, int N)
       TE(3, 3, 64, 4, 4);
       break;
     case 4: T0(3, 4); TE(3, 4, 160, 2, 2); break;
-    case 5: T0(3, 5); T(3, 5, 224, 3); T(3, 5, 224, 1); T(3, 5, 256, 2);
-      TE(3, 5, 224, 2, 2);
+    case 5: T0(3, 5); T(3, 5, 224, 4); T(3, 5, 224, 3); T(3, 5, 224, 1);
+      T(3, 5, 256, 2); TE(3, 5, 224, 2, 2);
       break;
     case 6: T0(3, 6); break;
     case 7: T0(3, 7); T(3, 7, 384, 1); break;
@@ -270,6 +291,9 @@ struct bfam_gpu_batch
     std::vector<int64_t> nwork_l;
     std::vector<int> grid;
     int ahead = 0; // L2 prefetch distance of one-buffer tiles (work items)
+    // no domain of the group has faces glued to another order, so level 0
+    // holds no element with a coarse-side face (launched without that pass)
+    bool level0_nc = false;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
   };
@@ -457,8 +481,9 @@ int issue_step(bfam_gpu_batch_t *b, int p)
       // hanging faces
       for (size_t l = 0; l < g.work.size(); ++l)
       {
-        t.launch(g.views[(p + s) & 1], g.work[l], (int)g.nwork_l[l], sp,
-                 g.hops.data(), g.grid[l], g.stream);
+        (l == 0 && g.level0_nc ? t.launch_nc : t.launch)(
+            g.views[(p + s) & 1], g.work[l], (int)g.nwork_l[l], sp,
+            g.hops.data(), g.grid[l], g.stream);
         CUDA_TRY(cudaGetLastError());
         ++launches;
       }
@@ -543,8 +568,9 @@ int issue_step_glued(bfam_gpu_batch_t *b, int p)
       sp.ahead = g.ahead;
       for (size_t l = 0; l < g.work.size(); ++l)
       {
-        t.launch(g.views[par], g.work[l], (int)g.nwork_l[l], sp,
-                 g.hops.data(), g.grid[l], g.stream);
+        (l == 0 && g.level0_nc ? t.launch_nc : t.launch)(
+            g.views[par], g.work[l], (int)g.nwork_l[l], sp, g.hops.data(),
+            g.grid[l], g.stream);
         CUDA_TRY(cudaGetLastError());
         ++launches;
       }
@@ -849,8 +875,13 @@ int bfam_gpu_batch_create(bfam_gpu_domain_t *const *doms, int ndom,
                   G.N, (long long)G.nwork);
     }
     int nl = 1;
+    G.level0_nc = true;
     for (int i : G.doms)
+    {
       nl = std::max(nl, doms[i]->nlevels);
+      if (doms[i]->nglued)
+        G.level0_nc = false;
+    }
     for (int l = 0; l < nl; ++l)
     {
       // level l of every domain, domain-major

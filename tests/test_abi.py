@@ -227,7 +227,7 @@ def test_tile_table():
                 assert threads % 32 == 0 and minb >= 1 and e >= 1
                 assert threads * e <= 1024
     assert bf.tile_elements(3, 3).count(1) == 3 and max(bf.tile_elements(3, 3)) == 4
-    assert len(bf.tile_shapes(3, 5)) == 5 and len(bf.tile_shapes(3, 7)) == 2
+    assert len(bf.tile_shapes(3, 5)) == 6 and len(bf.tile_shapes(3, 7)) == 2
     assert bf.lib().bfam_gpu_tile_count(3, 9) == 0
     a, b = C.c_int(), C.c_int()
     assert bf.lib().bfam_gpu_tile_shape(3, 5, 7, C.byref(a), C.byref(b)) == bf.BFAM_GPU_EINVAL
