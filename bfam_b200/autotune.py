@@ -35,7 +35,13 @@ def _brick_for(dim: int, elements: int, refine_prob: float = 0.2):
 
 
 def _key(gpu: str, dim: int, N: int, precision: int) -> str:
-    return f"{gpu}|dim{dim}|N{N}|prec{precision}"
+    """cache key: the GPU, the group, and the library's tile table for the
+    order (threads x register budget x elements per CTA of every tile), so
+    that a library with another table never reuses a tile index chosen
+    against the old one"""
+    table = "-".join(f"{t}x{m}x{e}" for (t, m), e in
+                     zip(tile_shapes(dim, N), tile_elements(dim, N)))
+    return f"{gpu}|dim{dim}|N{N}|prec{precision}|tiles:{table}"
 
 
 def load_cache(path: Path | None = None) -> dict:

@@ -232,3 +232,14 @@ def test_tile_table():
     a, b = C.c_int(), C.c_int()
     assert bf.lib().bfam_gpu_tile_shape(3, 5, 7, C.byref(a), C.byref(b)) == bf.BFAM_GPU_EINVAL
     assert bf.lib().bfam_gpu_tile_elements(3, 5, 7) == bf.BFAM_GPU_EINVAL
+
+
+def test_autotune_cache_key_names_the_tile_table():
+    """a cached tile index is only reused by a library with the same tile
+    table for the order (the key lists every tile's shape)"""
+    from bfam_b200 import autotune
+    k5 = autotune._key("B200", 3, 5, 1)
+    shapes = bf.tile_shapes(3, 5)
+    assert k5.startswith("B200|dim3|N5|prec1|tiles:")
+    assert k5.count("x") == 2 * len(shapes) and f"{shapes[0][0]}x{shapes[0][1]}x1" in k5
+    assert autotune._key("B200", 3, 3, 1) != autotune._key("B200", 3, 5, 1)
