@@ -52,24 +52,17 @@ __device__ __forceinline__ CT line_dx(const CT *x, const CT *Dl)
   return acc;
 }
 
-// Derivatives at two nodes of one strided line (along y or z): oa =
-// sum_m Da[m] x[STRIDE m], ob = sum_m Db[m] x[STRIDE m] (each value loaded
-// once).  With Db = Da only oa is formed.
-template <int N, int STRIDE, bool TWO, typename CT>
-__device__ __forceinline__ void line_d2(const CT *x, const CT *Da,
-                                        const CT *Db, CT &oa, CT &ob)
+// Derivative along y or z at one node: sum_m Dl[m] x[STRIDE m] over a
+// strided line of the tile.
+template <int N, int STRIDE, typename CT>
+__device__ __forceinline__ CT line_ds(const CT *x, const CT *Dl)
 {
   constexpr int Nq = N + 1;
-  oa = 0;
-  ob = 0;
+  CT acc = 0;
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-  {
-    const CT v = x[STRIDE * m];
-    oa += Da[m] * v;
-    if constexpr (TWO)
-      ob += Db[m] * v;
-  }
+    acc += Dl[m] * x[STRIDE * m];
+  return acc;
 }
 
 // s times the volume right-hand side at node (i, j, k):
@@ -96,14 +89,9 @@ __device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
   auto deriv = [&](int c, int ax, const CT *Dl) {
     if (ax == 0)
       return line_dx<N, CT>(qs + c * Np + Nq * (j + Nq * k), Dl);
-    CT acc, unused;
     if (ax == 1)
-      line_d2<N, Nq, false, CT>(qs + c * Np + i + Nq * Nq * k, Dl, Dl, acc,
-                                unused);
-    else
-      line_d2<N, Nq * Nq, false, CT>(qs + c * Np + i + Nq * j, Dl, Dl, acc,
-                                     unused);
-    return acc;
+      return line_ds<N, Nq, CT>(qs + c * Np + i + Nq * Nq * k, Dl);
+    return line_ds<N, Nq * Nq, CT>(qs + c * Np + i + Nq * j, Dl);
   };
 
   CT Dl[Nq];
