@@ -422,46 +422,85 @@ __device__ __forceinline__ void apply_half_s(const AT *A, int top, const T *v,
     out[m] = top ? o[N - m] : o[m];
 }
 
+// Position of face node idx = m0 + Nq m1 (m0 along face axis 0) in the
+// g-th Nfp-array of a face region (trace slots and flux jumps: g = f NTF +
+// slot; mortar jumps: g = fine rank NJ + slot).  In 3D at N = 7 the rows
+// and columns are XOR-swizzled by g: a thread per row (or column) in the
+// mortar line passes puts the lines of two consecutive arrays in a
+// half-warp, whose 8-byte accesses then fall on 16 distinct bank pairs,
+// where rows of 8 doubles would put them on 2 (rows) or 8 (columns); a
+// thread per face node (16 consecutive nodes: two whole rows of one array)
+// stays conflict-free.  The other orders keep the plain layout: at N = 5
+// every row offset 6 m1 and array offset 36 g is even in bank pairs, which
+// no permutation within a row fixes, and at N = 3 the analogous swizzle
+// (rows and columns XOR g mod 4) removed the conflicts but ran 2-3 %
+// slower.
+template <int DIM, int N>
+__device__ __forceinline__ int fpos(int g, int idx)
+{
+  if constexpr (DIM == 3 && N == 7)
+  {
+    const int m0 = idx & 7, m1 = idx >> 3, p = g & 1;
+    return 8 * (m1 ^ p) + (m0 ^ ((m1 >> 1) | (p << 2)));
+  }
+  else
+    return idx;
+}
+
+// Position of value i of line `line` of face array g: row m1 = line (ROWS)
+// or column m0 = line
+template <int DIM, int N, bool ROWS>
+__device__ __forceinline__ int line_pos(int g, int line, int i)
+{
+  return fpos<DIM, N>(g, ROWS ? i + (N + 1) * line : line + (N + 1) * i);
+}
+
 // line_apply with the operator in shared memory (OFFSET: interpolate the
 // variation along the line, as line_apply does for narrow types)
-template <int N, bool OFFSET, typename T, typename AT>
+template <int DIM, int N, bool ROWS, bool OFFSET, typename T, typename AT>
 __device__ __forceinline__ void line_apply_s(const AT *A, int top, double *x,
-                                             int stride)
+                                             int g, int line)
 {
   constexpr int Nq = N + 1;
-  const double ref = OFFSET ? x[0] : 0.0;
+  const double ref = OFFSET ? x[line_pos<DIM, N, ROWS>(g, line, 0)] : 0.0;
   T v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
-    v[i] = OFFSET ? T(x[i * stride] - ref) : T(x[i * stride]);
+  {
+    const double xi = x[line_pos<DIM, N, ROWS>(g, line, i)];
+    v[i] = OFFSET ? T(xi - ref) : T(xi);
+  }
   apply_half_s<N, T, AT>(A, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    x[m * stride] = OFFSET ? ref + double(v[m]) : double(v[m]);
+    x[line_pos<DIM, N, ROWS>(g, line, m)] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
-// In-place 1-D mortar operator pass on one line of a face array
-// x[m0 + Nq*m1] (stride 1: along face axis 0, stride Nq: along axis 1),
-// computed in T and stored back in double.  One thread owns one line.  An
-// interpolation in a type narrower than double is applied to the line minus
-// its first value, which is added back in double (interpolation reproduces
-// constants), so that the rounding is relative to the variation along the
-// line rather than to the values.
-template <int N, bool PROJ, typename T, typename CT>
+// In-place 1-D mortar operator pass on one line of face array g (x: the
+// array; ROWS: the row m1 = line, along face axis 0, else the column m0 =
+// line, along axis 1), computed in T and stored back in double.  One thread
+// owns one line.  An interpolation in a type narrower than double is applied
+// to the line minus its first value, which is added back in double
+// (interpolation reproduces constants), so that the rounding is relative to
+// the variation along the line rather than to the values.
+template <int DIM, int N, bool ROWS, bool PROJ, typename T, typename CT>
 __device__ __forceinline__ void line_apply(const DiffOp<N, CT> &op, int top,
-                                           double *x, int stride)
+                                           double *x, int g, int line)
 {
   constexpr int Nq = N + 1;
   constexpr bool OFFSET = !PROJ && sizeof(T) < sizeof(double);
-  const double ref = OFFSET ? x[0] : 0.0;
+  const double ref = OFFSET ? x[line_pos<DIM, N, ROWS>(g, line, 0)] : 0.0;
   T v[Nq];
 #pragma unroll
   for (int i = 0; i < Nq; ++i)
-    v[i] = OFFSET ? T(x[i * stride] - ref) : T(x[i * stride]);
+  {
+    const double xi = x[line_pos<DIM, N, ROWS>(g, line, i)];
+    v[i] = OFFSET ? T(xi - ref) : T(xi);
+  }
   apply_half<N, PROJ, T, CT>(op, top, v, v);
 #pragma unroll
   for (int m = 0; m < Nq; ++m)
-    x[m * stride] = OFFSET ? ref + double(v[m]) : double(v[m]);
+    x[line_pos<DIM, N, ROWS>(g, line, m)] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
 // Field of trace slot c on a face normal to axis ax: slots [0, DIM) are the

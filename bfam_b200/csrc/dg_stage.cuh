@@ -300,10 +300,13 @@ __device__ __forceinline__ void issue_element(const DomainView &d,
       // trees: the host refuses any other pairing or orientation)
       const int src_n = gmask<DIM, N>((ds.y >> 2) & 7, pn);
       const double *src = d.qin + (size_t)ds.x * Np + src_n;
-      double *dst = pt + f * NTF * Nfp + pn;
 #pragma unroll
       for (int c = 0; c < NTF; ++c)
-        cp_async8(dst + c * Nfp, src + trace_field<DIM>(f >> 1, c) * fs);
+      {
+        const int g = f * NTF + c;
+        cp_async8(pt + g * Nfp + fpos<DIM, N>(g, pn),
+                  src + trace_field<DIM>(f >> 1, c) * fs);
+      }
     }
     if (!S::TMA && pn == 0)
     {
@@ -454,11 +457,11 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int hp = (desc[f].y >> 8) & 7;
         const int c = r / ROWS, line = r % ROWS;
         const int half = pass == 0 ? (hp - 1) & 1 : (hp - 1) >> 1;
-        double *x = pt + (f * NTF + c) * Nfp;
+        const int g = f * NTF + c;
         if (pass == 0)
-          line_apply<N, false, CT, CT>(dop, half, x + Nq * line, 1);
+          line_apply<DIM, N, true, false, CT, CT>(dop, half, pt + g * Nfp, g, line);
         else
-          line_apply<N, false, CT, CT>(dop, half, x + line, Nq);
+          line_apply<DIM, N, false, false, CT, CT>(dop, half, pt + g * Nfp, g, line);
       }
       Sub<NT, EPC>::sync();
     }
@@ -484,7 +487,6 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int vm = gmask<DIM, N>(f, pn);
         const int pp = pn;
         CT dq[NTF], J[6];
-        double *x = pt + f * NTF * Nfp;
         // boundary faces: ghost state v+ = v-, S+ = -S- (free surface) or
         // q+ = 0 (absorbing)
         const bool free_surface = k == 3 && ((y >> 2) & 3) == 0;
@@ -492,7 +494,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         for (int c = 0; c < NTF; ++c)
         {
           const double qm = qs[trace_field<DIM>(f >> 1, c) * Np + vm];
-          const double qp = k != 3 ? x[c * Nfp + pp]
+          const int g = f * NTF + c;
+          const double qp = k != 3 ? pt[g * Nfp + fpos<DIM, N>(g, pp)]
                                    : (free_surface ? (c < DIM ? qm : -qm) : 0.0);
           dq[c] = CT(qp - qm);
         }
@@ -503,18 +506,21 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         {
           // rank of f among the fine faces (an element has at most DIM)
           const int fr = __popc(fine_mask & ((1 << f) - 1));
-          double *m = mj + fr * NJ * Nfp + pp;
 #pragma unroll
           for (int c = 0; c < NJ; ++c)
           {
             const int sl = jslot<DIM>(c);
             const CT v = sl < 3 ? sg * dq[DIM + sl] - J[sl] : J[sl] - dq[sl - 3];
-            m[c * Nfp] = double(v);
+            const int g = fr * NJ + c;
+            mj[g * Nfp + fpos<DIM, N>(g, pp)] = double(v);
           }
         }
 #pragma unroll
         for (int c = 0; c < NJ; ++c)
-          put_jump<CT>(x + c * Nfp + pp, J[jslot<DIM>(c)]);
+        {
+          const int g = f * NTF + c;
+          put_jump<CT>(pt + g * Nfp + fpos<DIM, N>(g, pp), J[jslot<DIM>(c)]);
+        }
       }
     }
   }
@@ -532,7 +538,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
 #pragma unroll
       for (int p = 0; p < NPC; ++p)
         sum += mb[(p * NJ + c) * Nfp];
-      put_jump<CT>(pt + (f * NTF + c) * Nfp + pn, CT(sum));
+      const int g = f * NTF + c;
+      put_jump<CT>(pt + g * Nfp + fpos<DIM, N>(g, pn), CT(sum));
     }
   }
 
@@ -545,9 +552,9 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
     {
       const int fr = w / (NJ * ROWS), r = w % (NJ * ROWS);
       const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
-      const int c = r / ROWS, line = r % ROWS;
-      line_apply_s<N, false, double, double>(
-          sPb, (hp - 1) & 1, mj + (fr * NJ + c) * Nfp + Nq * line, 1);
+      const int g = fr * NJ + r / ROWS, line = r % ROWS;
+      line_apply_s<DIM, N, true, false, double, double>(
+          sPb, (hp - 1) & 1, mj + g * Nfp, g, line);
     }
     Sub<NT, EPC>::sync();
     if (DIM == 3)
@@ -556,18 +563,18 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       {
         const int fr = w / (NJ * Nq), r = w % (NJ * Nq);
         const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
-        const int c = r / Nq, col = r % Nq;
-        line_apply_s<N, false, double, double>(
-            sPb, (hp - 1) >> 1, mj + (fr * NJ + c) * Nfp + col, Nq);
+        const int g = fr * NJ + r / Nq, col = r % Nq;
+        line_apply_s<DIM, N, false, false, double, double>(
+            sPb, (hp - 1) >> 1, mj + g * Nfp, g, col);
       }
       Sub<NT, EPC>::sync();
     }
     for (int w = t; w < nfine * NJ * Nfp; w += NT)
     {
       const int fr = w / (NJ * Nfp), r = w % (NJ * Nfp);
-      const int f = nth_bit(fine_mask, fr);
+      const int f = nth_bit(fine_mask, fr), g = fr * NJ + r / Nfp;
       d.mbuf[(size_t)d.fslot[(size_t)e * NF + f] * NJ * Nfp + r] =
-          mj[fr * NJ * Nfp + r];
+          mj[g * Nfp + fpos<DIM, N>(g, r % Nfp)];
     }
   }
   Sub<NT, EPC>::sync();
@@ -605,11 +612,12 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       const int pn = DIM == 3 ? (ax == 0 ? j + Nq * k
                                          : (ax == 1 ? i + Nq * k : i + Nq * j))
                               : (ax == 0 ? j : i);
-      const double *jp = pt + (2 * ax + side) * NTF * Nfp + pn;
+      const int g0 = (2 * ax + side) * NTF;
       CT J[6] = {0, 0, 0, 0, 0, 0}, lc[NFLD];
 #pragma unroll
       for (int c = 0; c < NJ; ++c)
-        J[jslot<DIM>(c)] = get_jump<CT>(jp + c * Nfp);
+        J[jslot<DIM>(c)] =
+            get_jump<CT>(pt + (g0 + c) * Nfp + fpos<DIM, N>(g0 + c, pn));
       lift_face<DIM, CT>(J, ax, side ? CT(1) : CT(-1), lfac[ax], me, lc);
 #pragma unroll
       for (int c = 0; c < NFLD; ++c)
