@@ -179,9 +179,9 @@ template <int DIM, int N> struct Shape
   // at most DIM faces on the fine side of a hanging face (those on its
   // parent's boundary)
   static constexpr int SM_MJ = DIM * NJ * Nfp + (DIM * NJ * Nfp) % 2;
-  // differentiation matrix, bottom-half mortar interpolation and projection
-  // (Nq*Nq entries each, one double slot per entry)
-  static constexpr int SM_IP = 3 * Nq * Nq + (Nq % 2);
+  // differentiation matrix (Nq*Nq entries, one double slot per entry): the
+  // volume pass reads its rows per node, at thread-dependent rows
+  static constexpr int SM_IP = Nq * Nq + (Nq % 2);
   // precision form only: FP32 copy of q minus the element's first node,
   // after the mbarriers
   static constexpr int SM_QF = (NFLD * Np + 3) / 4 * 2;
@@ -396,32 +396,6 @@ __device__ __forceinline__ void apply_half(const DiffOp<N, CT> &op, int top,
     out[m] = top ? o[N - m] : o[m];
 }
 
-// out = A v with A(m, i) = A[m + Nq i] a bottom-half mortar operator held in
-// shared memory (AT: its stored type), or its top-half reflection when
-// top != 0 (see apply_half).
-template <int N, typename T, typename AT>
-__device__ __forceinline__ void apply_half_s(const AT *A, int top, const T *v,
-                                             T *out)
-{
-  constexpr int Nq = N + 1;
-  T vr[Nq], o[Nq];
-#pragma unroll
-  for (int i = 0; i < Nq; ++i)
-    vr[i] = top ? v[N - i] : v[i];
-#pragma unroll
-  for (int m = 0; m < Nq; ++m)
-  {
-    T s = 0;
-#pragma unroll
-    for (int i = 0; i < Nq; ++i)
-      s += T(A[m + Nq * i]) * vr[i];
-    o[m] = s;
-  }
-#pragma unroll
-  for (int m = 0; m < Nq; ++m)
-    out[m] = top ? o[N - m] : o[m];
-}
-
 // Position of face node idx = m0 + Nq m1 (m0 along face axis 0) in the
 // g-th Nfp-array of a face region (trace slots and flux jumps: g = f NTF +
 // slot; mortar jumps: g = fine rank NJ + slot).  In 3D at N = 7 the rows
@@ -453,27 +427,6 @@ template <int DIM, int N, bool ROWS>
 __device__ __forceinline__ int line_pos(int g, int line, int i)
 {
   return fpos<DIM, N>(g, ROWS ? i + (N + 1) * line : line + (N + 1) * i);
-}
-
-// line_apply with the operator in shared memory (OFFSET: interpolate the
-// variation along the line, as line_apply does for narrow types)
-template <int DIM, int N, bool ROWS, bool OFFSET, typename T, typename AT>
-__device__ __forceinline__ void line_apply_s(const AT *A, int top, double *x,
-                                             int g, int line)
-{
-  constexpr int Nq = N + 1;
-  const double ref = OFFSET ? x[line_pos<DIM, N, ROWS>(g, line, 0)] : 0.0;
-  T v[Nq];
-#pragma unroll
-  for (int i = 0; i < Nq; ++i)
-  {
-    const double xi = x[line_pos<DIM, N, ROWS>(g, line, i)];
-    v[i] = OFFSET ? T(xi - ref) : T(xi);
-  }
-  apply_half_s<N, T, AT>(A, top, v, v);
-#pragma unroll
-  for (int m = 0; m < Nq; ++m)
-    x[line_pos<DIM, N, ROWS>(g, line, m)] = OFFSET ? ref + double(v[m]) : double(v[m]);
 }
 
 // In-place 1-D mortar operator pass on one line of face array g (x: the

@@ -96,8 +96,8 @@ template <typename CT> __device__ __forceinline__ CT get_jump(const double *slot
 // Shared-memory layout of one CTA (in doubles, every region 16-byte
 // aligned).  NBUF element buffers (state, dq, face traces / flux jumps, face
 // flux constants) let the loads of the next element fly
-// while the current one is computed; the mortar scratch, the 1-D operators,
-// the mbarriers (q and dq per buffer) and the precision form's FP32 tile are
+// while the current one is computed; the mortar scratch, the differentiation
+// matrix, the mbarriers (q and dq per buffer) and the precision form's FP32 tile are
 // single.
 template <int DIM, int N, typename CT, int NBUF, bool DQS = true> struct Tile
 {
@@ -383,7 +383,6 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
   uint64_t *bar_q = tb.bq, *bar_dq = tb.bdq;
   double *mj = smem + T::OFF_MJ; // [DIM][NJ][Nfp] coarse-side jumps, by fine rank
   const CT *sD = reinterpret_cast<const CT *>(smem + T::OFF_OPS); // D
-  const double *sPb = smem + T::OFF_OPS + 2 * Nq * Nq; // projection
   // the volume pass's copy of q: q itself in the plain form; in the
   // precision form FP32 q minus the element's first node per field (the
   // derivative of a constant is zero), so that rounding is relative to the
@@ -553,8 +552,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
       const int fr = w / (NJ * ROWS), r = w % (NJ * ROWS);
       const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
       const int g = fr * NJ + r / ROWS, line = r % ROWS;
-      line_apply_s<DIM, N, true, false, double, double>(
-          sPb, (hp - 1) & 1, mj + g * Nfp, g, line);
+      line_apply<DIM, N, true, true, double, CT>(
+          dop, (hp - 1) & 1, mj + g * Nfp, g, line);
     }
     Sub<NT, EPC>::sync();
     if (DIM == 3)
@@ -564,8 +563,8 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
         const int fr = w / (NJ * Nq), r = w % (NJ * Nq);
         const int hp = (desc[nth_bit(fine_mask, fr)].y >> 8) & 7;
         const int g = fr * NJ + r / Nq, col = r % Nq;
-        line_apply_s<DIM, N, false, false, double, double>(
-            sPb, (hp - 1) >> 1, mj + g * Nfp, g, col);
+        line_apply<DIM, N, false, true, double, CT>(
+            dop, (hp - 1) >> 1, mj + g * Nfp, g, col);
       }
       Sub<NT, EPC>::sync();
     }
@@ -601,7 +600,7 @@ __device__ __forceinline__ void compute_element(const DomainView &d,
     // jumps of the faces this node lies on (at most one per axis, in face
     // order); widened to FP64 once for the update
     CT rv[NFLD];
-    volume_node<DIM, N, CT>(qv, sD, me, s, i, j, k, rv);
+    volume_node<DIM, N, CT>(qv, sD, dop, me, s, i, j, k, rv);
 #pragma unroll
     for (int ax = 0; ax < DIM; ++ax)
     {
@@ -689,17 +688,13 @@ __device__ __forceinline__ void stage_loop(const Item &item, int n,
     for (int i = 0; i < 2 * NBUF; ++i)
       mbar_init(&bar[i], 1);
   }
-  // 1-D operators into shared memory (indexed per thread later)
+  // the differentiation matrix into shared memory (rows indexed per
+  // thread in the volume pass; the mortar operators are read from the
+  // parameter bank at unrolled indices)
   {
     CT *sD = reinterpret_cast<CT *>(smem + T::OFF_OPS);
-    CT *sIb = reinterpret_cast<CT *>(smem + T::OFF_OPS + Nq * Nq);
-    double *sPb = smem + T::OFF_OPS + 2 * Nq * Nq;
     for (int w = lt; w < Nq * Nq; w += NT)
-    {
       sD[w] = dop.D[w];
-      sIb[w] = dop.Ib[w];
-      sPb[w] = dop.Pb[w];
-    }
   }
   SB::sync();
   int idx = (int)blockIdx.x * EPC + SB::id();

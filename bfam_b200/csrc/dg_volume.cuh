@@ -65,15 +65,36 @@ __device__ __forceinline__ CT line_ds(const CT *x, const CT *Dl)
   return acc;
 }
 
+// Axes whose row of the differentiation matrix a node reads from the
+// kernel's parameter space (constant cache) rather than from its shared
+// memory copy (bit 0: x, 1: y, 2: z).  Shared 8-byte loads cost two L1
+// wavefronts per warp however few distinct rows a warp reads, and the L1
+// data pipe is the busiest unit of the stage kernel; constant-cache reads
+// cost nothing there but serialise over the distinct rows of a warp.  A
+// warp's nodes share k at N = 5 (but for the last warp) and N = 7, and span
+// two k at N = 3.  Measured per shape (G DOF-updates/s against shared
+// rows): z alone +0.6 % (FP64) and +1 % (FP32) at N = 7, where all three
+// axes (eight distinct i) lost 3 and 9 %; all three axes +0.8 % at N = 3
+// (four distinct rows) in both forms and +0.6 % at N = 5 in FP64, where
+// FP32 lost 3.5 % with them and gains 0.4 % with z alone.  Other shapes
+// keep the shared copy.
+template <int DIM, int N, typename CT> constexpr int dparam_axes()
+{
+  if (DIM != 3)
+    return 0;
+  return N == 3 ? 7 : N == 5 ? (sizeof(CT) == 8 ? 7 : 4) : N == 7 ? 4 : 0;
+}
+
 // s times the volume right-hand side at node (i, j, k):
 //   rho dv/dt = div S,  dS/dt = lambda div(v) I + mu (grad v + grad v^T)
 // with the derivative along each axis the 1-D LGL differentiation matrix
 // applied along that axis -- the BFAM_KRON_IXIXA / IXAXI / AXIXI
 // contractions of src/bfam.c:3519-3624 evaluated at one node.  qs is the
 // element's state tile in CT, sD the column-major D(i,m) = sD[i + Nq m], both
-// in shared memory.
+// in shared memory, dop the same operators in the kernel's parameter space.
 template <int DIM, int N, typename CT>
 __device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
+                                            const DiffOp<N, CT> &dop,
                                             const ElemData &me, double s, int i,
                                             int j, int k, CT *rv)
 {
@@ -94,12 +115,13 @@ __device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
     return line_ds<N, Nq * Nq, CT>(qs + c * Np + i + Nq * j, Dl);
   };
 
+  constexpr int PA = dparam_axes<DIM, N, CT>();
   CT Dl[Nq];
   // x
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = sD[i + Nq * m];
+      Dl[m] = (PA & 1) ? dop.D[i + Nq * m] : sD[i + Nq * m];
     const CT r = CT(s * me.rx);
     const CT dvx = r * deriv(0, 0, Dl), dvy = r * deriv(1, 0, Dl);
     if (DIM == 3)
@@ -127,7 +149,7 @@ __device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = sD[j + Nq * m];
+      Dl[m] = (PA & 2) ? dop.D[j + Nq * m] : sD[j + Nq * m];
     const CT r = CT(s * me.ry);
     const CT dvx = r * deriv(0, 1, Dl), dvy = r * deriv(1, 1, Dl);
     if (DIM == 3)
@@ -156,7 +178,7 @@ __device__ __forceinline__ void volume_node(const CT *qs, const CT *sD,
   {
 #pragma unroll
     for (int m = 0; m < Nq; ++m)
-      Dl[m] = sD[k + Nq * m];
+      Dl[m] = (PA & 4) ? dop.D[k + Nq * m] : sD[k + Nq * m];
     const CT r = CT(s * me.rz);
     const CT dvx = r * deriv(0, 2, Dl), dvy = r * deriv(1, 2, Dl),
              dvz = r * deriv(2, 2, Dl);
