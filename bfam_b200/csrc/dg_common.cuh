@@ -410,7 +410,7 @@ __device__ __forceinline__ void apply_half(const DiffOp<N, CT> &op, int top,
 // (rows and columns XOR g mod 4) removed the conflicts but ran 2-3 %
 // slower.
 template <int DIM, int N>
-__device__ __forceinline__ int fpos(int g, int idx)
+__host__ __device__ __forceinline__ int fpos(int g, int idx)
 {
   if constexpr (DIM == 3 && N == 7)
   {
@@ -424,7 +424,7 @@ __device__ __forceinline__ int fpos(int g, int idx)
 // Position of value i of line `line` of face array g: row m1 = line (ROWS)
 // or column m0 = line
 template <int DIM, int N, bool ROWS>
-__device__ __forceinline__ int line_pos(int g, int line, int i)
+__host__ __device__ __forceinline__ int line_pos(int g, int line, int i)
 {
   return fpos<DIM, N>(g, ROWS ? i + (N + 1) * line : line + (N + 1) * i);
 }
